@@ -1,0 +1,147 @@
+"""3-D scalar Burgers on a periodic Kuhn-cube mesh, assembled through the runner API.
+
+This is the calling pattern of examples/3d_scalar_burgers_equation.go:168-471 with the full strong-form
+right-hand side: bindings for state, geometry, face data and reference matrices; FP64 geometry and face
+maps computed on the GPU; the FaceConnector exchange fused into a gather map; one `rhsStage` kernel per
+LSERK4 stage.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import mesh as M
+from .element import Element
+from .runner import (Config, Float32, Float64, INT32, INT64, Runner, Scalar, Temp, Input)
+from ._lib import check, lib
+
+import ctypes as C
+
+# Carpenter-Kennedy five-stage LSERK4 (examples/3d_scalar_burgers_equation.go:138-151)
+RK4A = (0.0, -567301805773.0 / 1357537059087.0, -2404267990393.0 / 2016746695238.0,
+        -3550918686646.0 / 2091501179385.0, -1275806237668.0 / 842570457699.0)
+RK4B = (1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
+        1720146321549.0 / 2090206949498.0, 3134564353537.0 / 4481467310338.0,
+        2277821191437.0 / 14882151754819.0)
+
+DEFAULT_SEED = 20261203
+GEO = ("Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz")
+FACE = ("nx", "ny", "nz", "Fscale")
+
+
+class UniformStream:
+    """Sequential splitmix64 uniforms drawn in blocks from the library."""
+
+    def __init__(self, seed: int, block: int = 4096):
+        self.seed, self.block, self.buf, self.pos = seed, block, M.splitmix_uniform(seed, block), 0
+
+    def uniform(self) -> float:
+        if self.pos == len(self.buf):
+            self.buf = M.splitmix_uniform(self.seed, len(self.buf) * 2)
+        v = float(self.buf[self.pos])
+        self.pos += 1
+        return v
+
+    def normal(self) -> float:
+        u1 = 1.0 - self.uniform()
+        u2 = self.uniform()
+        return math.sqrt(-2.0 * math.log(u1)) * math.cos(2.0 * math.pi * u2)
+
+
+def random_modes(seed: int, nmodes: int = 8, kmax: int = 3, sigma: float = 0.1) -> np.ndarray:
+    """Rows (kx, ky, kz, a, phi): integer k in [-kmax,kmax]^3 with 0 < |k| <= kmax by rejection,
+    a ~ N(0, sigma^2), phi ~ U[0, 2 pi)."""
+    rng = UniformStream(seed)
+    rows = []
+    for _ in range(nmodes):
+        while True:
+            k = [int(math.floor(rng.uniform() * (2 * kmax + 1))) - kmax for _ in range(3)]
+            k2 = sum(v * v for v in k)
+            if 0 < k2 <= kmax * kmax:
+                break
+        a = sigma * rng.normal()
+        phi = 2.0 * math.pi * rng.uniform()
+        rows.append([k[0], k[1], k[2], a, phi])
+    return np.array(rows, dtype=np.float64)
+
+
+class BurgersProblem:
+    """Device-resident Burgers problem of order N on an n^3 x 6 Kuhn mesh with nslab x-slab partitions."""
+
+    def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
+                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None):
+        self.N, self.n, self.nslab = N, n, nslab
+        self.dtype = np.dtype(dtype)
+        dt_code = Float64 if self.dtype == np.float64 else Float32
+        el = self.el = Element(N)
+        Np, Nfp = el.Np, el.Nfp
+        NF = 4 * Nfp
+        VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)
+        self.EToV, self.EToP = EToV, EToP
+        EToE, EToF = M.ti_connect3d(EToVp)
+        K = self.K = EToV.shape[0]
+        self.Kpart = [K // nslab] * nslab
+        r = self.runner = Runner(Config(K=self.Kpart), stream=stream)
+        sn = el.ShortName
+        params = [Temp(nm).Type(dt_code).Size(K * Np) for nm in ("u", "uNext", "resu", "X", "Y", "Z") + GEO]
+        params += [Temp(nm).Type(dt_code).Size(K * NF) for nm in FACE]
+        params += [Temp("gmap").Type(INT32).Size(K * NF), Temp("vmapP").Type(INT64).Size(K * NF)]
+        params += [Input(f"{m}_{sn}").Bind(getattr(el, m)).ToMatrix().Static() for m in ("Dr", "Ds", "Dt", "LIFT")]
+        params += [Input("Fmask").Bind(el.Fmask.astype(np.float64)).ToMatrix().DeviceMemType(INT32)]
+        params += [Scalar("a").Type(Float64), Scalar("b").Type(Float64), Scalar("dt").Type(Float64)]
+        r.DefineBindings(*params)
+        r.AllocateDevice()
+        # FP64 geometry, normals and periodic VmapP on the GPU
+        names = ["X", "Y", "Z", *GEO, None, "nx", "ny", "nz", None, "Fscale", None, "vmapP"]
+        carr = (C.c_char_p * 20)(*[None if v is None else v.encode() for v in names])
+        hmin = C.c_double()
+        _pd = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        _pi = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
+        check(lib().dgk_setup_geometry(r._h, el._h, len(VX), _pd(VX), _pd(VY), _pd(VZ), _pi(EToV), _pi(EToE),
+                                       _pi(EToF), 2.0, carr, C.byref(hmin)), r._h)
+        self.hmin = hmin.value
+        # FaceConnector pick/place fused into one gather map over the state array's partition offsets
+        self.vmapP = np.zeros(K * NF, dtype=np.int64)
+        r.CopyFromDevice("vmapP", self.vmapP)
+        self.node_off = r.GetOffsets("u")
+        self.gmap = M.face_gather_map(K, 4, Nfp, Np, self.vmapP, EToP, self.node_off)
+        r.CopyToDevice("gmap", self.gmap)
+        # initial condition
+        if u0_host is not None:
+            r.CopyToDevice("u", np.ascontiguousarray(u0_host, dtype=self.dtype).reshape(-1))
+        else:
+            kinds = {"sine": (0, 0.0, 0.5), "shock": (0, 0.5, 1.0), "smooth": (1, 0.5, 0.25), "modes": (2, 0.5, 0.0)}
+            kind, mean, amp = kinds[u0]
+            modes = random_modes(seed) if kind == 2 else np.zeros((0, 5))
+            check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, len(modes), _pd(modes)), r._h)
+        self.u0 = self.get("u")
+        self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))
+        fixed = ["u", "uNext", "resu", *GEO, *FACE, "gmap", f"Dr_{sn}", f"Ds_{sn}", f"Dt_{sn}", f"LIFT_{sn}", "Fmask"]
+        r.ConfigureKernel("rhsStage", *[r.Param(p) for p in fixed], r.Param("a"), r.Param("b"), r.Param("dt"))
+        r.BuildKernel(f"rhsStage(conservative={conservative})", "rhsStage")
+        self.stage = 0
+
+    @property
+    def dofs(self) -> int:
+        return self.K * self.el.Np
+
+    def get(self, name: str) -> np.ndarray:
+        n = self.K * (self.el.Np if name not in FACE + ("gmap", "vmapP") else 4 * self.el.Nfp)
+        dt = {"gmap": np.int32, "vmapP": np.int64}.get(name, self.dtype)
+        out = np.zeros(n, dtype=dt)
+        self.runner.CopyFromDevice(name, out)
+        return out
+
+    def set(self, name: str, host: np.ndarray):
+        self.runner.CopyToDevice(name, np.ascontiguousarray(host))
+
+    def run_stages(self, nstages: int):
+        """Advance by nstages LSERK4 stages (stage index continues across calls)."""
+        for _ in range(nstages):
+            s = self.stage % 5
+            self.runner.ExecuteKernel("rhsStage", RK4A[s], RK4B[s], self.dt)
+            self.stage += 1
+
+    def free(self):
+        self.runner.Free()

@@ -1,0 +1,90 @@
+// sm_100a kernels of the tet-DG right-hand side (plain FP64 / FP32 forms).
+//
+// Data layout (HBM): every node array is element-contiguous, node n of element k at k*Np + n, and every
+// face array holds 4*Nfp face points per element in face-major order (the reference layout of
+// element/physical_element.go:29-46).  Work is cut into tiles of up to TE consecutive elements of one
+// partition; a tile's slice of each array is one contiguous run, so it is read with coalesced vector
+// loads.  A persistent grid of CTAs walks the tile list; each CTA stages the reference matrices
+// (Dr, Ds, Dt, LIFT) in shared memory once and reads them with warp-uniform broadcasts.
+//
+// Thread mapping for the element-local matrix products: thread t owns element e = t % TE of the tile and
+// row group g = t / TE (RG consecutive rows), so the 32 lanes of a warp hold 32 elements and share every
+// matrix entry they read.  Element-major tiles in shared memory use an odd row stride, which keeps the
+// strided per-element reads of a warp free of bank conflicts.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dgk {
+
+struct Tile {
+  int64_t node_base;  // value index of the tile's first element in node arrays (Np values per element)
+  int64_t face_base;  // value index of the tile's first element in face arrays (4*Nfp values per element)
+  int32_t nelem;      // elements in this tile (<= TE)
+  int32_t part;       // partition (or instance) the tile belongs to
+};
+
+// Status word codes written by kernels (never a trap: the host reads the word and reports).
+enum : int { kStatusOk = 0, kStatusBadGather = 1 };
+
+template <int N>
+struct Order {
+  static constexpr int NP = (N + 1) * (N + 2) * (N + 3) / 6;
+  static constexpr int NFP = (N + 1) * (N + 2) / 2;
+  static constexpr int NF = 4 * NFP;
+  static constexpr int NPS = NP | 1;  // odd shared-memory strides
+  static constexpr int NFS = NF | 1;
+};
+
+// Launch shape per order: TE elements per tile, RG rows per thread in the matrix products.
+template <int N>
+struct Shape;
+template <> struct Shape<1> { static constexpr int TE = 128, RG = 2; };
+template <> struct Shape<2> { static constexpr int TE = 64, RG = 5; };
+template <> struct Shape<3> { static constexpr int TE = 64, RG = 5; };
+template <> struct Shape<4> { static constexpr int TE = 32, RG = 5; };
+template <> struct Shape<5> { static constexpr int TE = 32, RG = 7; };
+template <> struct Shape<6> { static constexpr int TE = 32, RG = 7; };
+template <> struct Shape<7> { static constexpr int TE = 32, RG = 8; };
+
+template <int N>
+struct Cfg {
+  using O = Order<N>;
+  static constexpr int TE = Shape<N>::TE, RG = Shape<N>::RG;
+  static constexpr int G = (O::NP + RG - 1) / RG;
+  static constexpr int THREADS = TE * G;
+};
+
+// Arguments of the fused stage / RHS kernels.  Matrices are row-major in the kernel's type.
+template <typename T>
+struct RhsArgs {
+  const Tile *tiles;
+  int ntiles;
+  const T *u_in;  // state read by this stage (also the neighbour traces)
+  T *u_out;       // state written by this stage (ping-pong partner of u_in)
+  T *resu;        // LSERK residual, updated in place
+  T *rhs_out;     // RHS-only mode: the right-hand side
+  const T *geo[9];       // rx, ry, rz, sx, sy, sz, tx, ty, tz per node
+  const T *face[4];      // nx, ny, nz, Fscale per face point
+  const int32_t *gmap;   // neighbour value index per face point (fused FaceConnector exchange)
+  int64_t n_u_values;    // bound of gmap entries
+  const T *Dmat;         // [3][NP][NP] Dr, Ds, Dt
+  const T *LIFT;         // [NP][NF]
+  const int32_t *fmask;  // [NF]
+  T a, b, dt;            // LSERK stage coefficients
+  int conservative;      // 0: -u (ux+uy+uz) (reference form), 1: -div(u^2/2 (1,1,1))
+  int *status;
+};
+
+template <typename T>
+struct DiffArgs {
+  const Tile *tiles;
+  int ntiles;
+  const T *u;
+  const T *geo[9];
+  T *out[3];   // differentiate: DuDx, DuDy, DuDz;  computeRHS: out[0] = rhsu
+  int mode;    // 0 = differentiate, 1 = reference volume-only computeRHS
+  const T *Dmat;
+};
+
+}  // namespace dgk

@@ -1,0 +1,50 @@
+// Host-side declarations of the kernel launchers (kernels.cu, setup.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "dg_kernels.cuh"
+
+namespace dgk {
+
+struct LaunchInfo {
+  int grid = 0, threads = 0, smem = 0, per_sm = 0;
+};
+
+template <typename T>
+void launch_rhs(int N, const RhsArgs<T> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info);
+template <typename T>
+void launch_diff(int N, const DiffArgs<T> &A, int num_sms, cudaStream_t st, LaunchInfo *info);
+template <typename T>
+void launch_update(const Tile *tiles, int ntiles, int np, T *u, T *resu, const T *rhs, double c0, double c1, double c2,
+                   int mode, int num_sms, cudaStream_t st);
+int tile_elems(int N);
+
+// Generic MATMUL_<M> over partitions: out[e*rows + i] (+)= sum_j M[i][j] in[e*cols + j].
+template <typename T>
+void launch_matmul(const T *M_rowmajor, int rows, int cols, const T *in, T *out, const int64_t *d_in_off,
+                   const int64_t *d_out_off, const int64_t *d_K, int npart, int64_t kmax, int add, cudaStream_t st);
+
+// FP64 geometry setup (setup.cu).  Packed element-contiguous outputs (K*Np or K*4Nfp values).
+struct GeoSetup {
+  int N, Np, Nfp;
+  int64_t K;
+  const double *VX, *VY, *VZ;  // device
+  const int64_t *EToV;         // device, K*4
+  const int64_t *EToE, *EToF;  // device, K*4
+  const double *rst;           // device, 3*Np (r, s, t)
+  const double *Dr, *Ds, *Dt;  // device, Np*Np row-major
+  const int *fmask;            // device, 4*Nfp
+  double period;
+};
+// which: 0..2 = X,Y,Z; 3..11 = rx,ry,rz,sx,sy,sz,tx,ty,tz; 12 = J (node arrays);
+//        13..17 = nx, ny, nz, sJ, Fscale (face arrays)
+void launch_geo_field(const GeoSetup &g, int which, double *out, cudaStream_t st);
+// vmapM (global node id of each face point) and vmapP (matched neighbour node) as int64.
+void launch_build_maps(const GeoSetup &g, int64_t *vmapM, int64_t *vmapP, cudaStream_t st);
+// Smallest node-pair distance above 1e-12 (as an ordered 64-bit pattern of a positive double).
+void launch_hmin(const GeoSetup &g, unsigned long long *dmin, cudaStream_t st);
+template <typename T>
+void launch_field(T *u, const T *X, const T *Y, const T *Z, int64_t n, int kind, double mean, double amp,
+                  const double *modes, int nmodes, cudaStream_t st);
+
+}  // namespace dgk

@@ -1,0 +1,160 @@
+// Mesh-side setup on the host: the periodic Kuhn-cube generator, tiConnect3D face matching, the
+// FaceConnector pick/place lists and their fused one-address-space gather map.
+#include "mesh.hpp"
+
+#include <algorithm>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+
+namespace dgk {
+
+// Corner offsets (x,y,z bits) of the 6 Kuhn tets of a unit cube, all containing the diagonal
+// (0,0,0)-(1,1,1), in the order and orientation (J > 0) of utils/mesh_test_helpers.go:353-366.
+static const int kKuhn[6][4][3] = {
+    {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {1, 1, 1}}, {{0, 0, 0}, {1, 1, 0}, {0, 1, 0}, {1, 1, 1}},
+    {{0, 0, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}}, {{0, 0, 0}, {0, 1, 1}, {0, 0, 1}, {1, 1, 1}},
+    {{0, 0, 0}, {1, 0, 1}, {1, 0, 0}, {1, 1, 1}}, {{0, 0, 0}, {0, 1, 0}, {0, 1, 1}, {1, 1, 1}}};
+
+void kuhn_mesh(int n, int nslab, double lo, double hi, double *VX, double *VY, double *VZ, int64_t *EToV,
+               int64_t *EToVp, int64_t *EToP) {
+  if (n < 2) throw std::invalid_argument("Kuhn mesh needs n >= 2");
+  if (nslab < 1 || n % nslab) throw std::invalid_argument("n must be a multiple of the slab count");
+  const int64_t m = n + 1;
+  const double h = (hi - lo) / n;
+  for (int64_t i = 0; i < m; ++i)
+    for (int64_t j = 0; j < m; ++j)
+      for (int64_t k = 0; k < m; ++k) {
+        const int64_t v = (i * m + j) * m + k;
+        VX[v] = lo + h * (double)i;
+        VY[v] = lo + h * (double)j;
+        VZ[v] = lo + h * (double)k;
+      }
+  const int per = n / nslab;
+  for (int64_t i = 0; i < n; ++i)
+    for (int64_t j = 0; j < n; ++j)
+      for (int64_t k = 0; k < n; ++k) {
+        const int64_t cube = (i * n + j) * n + k;
+        for (int t = 0; t < 6; ++t) {
+          const int64_t e = cube * 6 + t;
+          for (int c = 0; c < 4; ++c) {
+            const int64_t gi = i + kKuhn[t][c][0], gj = j + kKuhn[t][c][1], gk = k + kKuhn[t][c][2];
+            EToV[e * 4 + c] = (gi * m + gj) * m + gk;
+            EToVp[e * 4 + c] = ((gi % n) * n + (gj % n)) * n + (gk % n);
+          }
+          EToP[e] = i / per;
+        }
+      }
+}
+
+// Faces {0,1,2}, {0,1,3}, {1,2,3}, {0,2,3} keyed by their sorted vertex triple
+// (element/library/gonudg/ticonnect3d.go:24-102).  Equal keys are linked pairwise in sorted order.
+void ti_connect3d(int64_t K, const int64_t *EToV, int64_t *EToE, int64_t *EToF) {
+  static const int fv[4][3] = {{0, 1, 2}, {0, 1, 3}, {1, 2, 3}, {0, 2, 3}};
+  int64_t nn = 0;
+  for (int64_t i = 0; i < 4 * K; ++i) nn = std::max(nn, EToV[i] + 1);
+  struct Key {
+    int64_t id, slot;
+  };
+  std::vector<Key> keys((size_t)(4 * K));
+  for (int64_t e = 0; e < K; ++e)
+    for (int f = 0; f < 4; ++f) {
+      int64_t v[3] = {EToV[e * 4 + fv[f][0]], EToV[e * 4 + fv[f][1]], EToV[e * 4 + fv[f][2]]};
+      std::sort(v, v + 3);
+      keys[(size_t)(e * 4 + f)] = {(v[0] * nn + v[1]) * nn + v[2], e * 4 + f};
+    }
+  std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
+    return a.id != b.id ? a.id < b.id : a.slot < b.slot;
+  });
+  for (int64_t e = 0; e < K; ++e)
+    for (int f = 0; f < 4; ++f) {
+      EToE[e * 4 + f] = e;
+      EToF[e * 4 + f] = f;
+    }
+  for (size_t i = 0; i + 1 < keys.size(); ++i) {
+    if (keys[i].id != keys[i + 1].id) continue;
+    const int64_t a = keys[i].slot, b = keys[i + 1].slot;
+    EToE[a] = b / 4;
+    EToF[a] = b % 4;
+    EToE[b] = a / 4;
+    EToF[b] = a % 4;
+  }
+}
+
+// NewFaceConnector + BuildIndices + Verify (utils/face_connector.go:43-253).  Local element numbers
+// follow increasing global id inside each partition.
+FaceConnector face_connector(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmapP, const int64_t *EToP,
+                             int npart) {
+  if (K <= 0 || Nfaces <= 0 || Nfp <= 0 || Np <= 0) throw std::invalid_argument("invalid dimensions");
+  int P = 0;
+  for (int64_t e = 0; e < K; ++e) {
+    if (EToP[e] < 0) throw std::invalid_argument("negative partition id");
+    P = std::max<int>(P, (int)EToP[e] + 1);
+  }
+  if (npart > 0 && P != npart) throw std::invalid_argument("EToP partition count does not match npart");
+  FaceConnector fc;
+  fc.nparts = P;
+  fc.elems.assign(P, 0);
+  std::vector<int64_t> local((size_t)K);
+  for (int64_t e = 0; e < K; ++e) local[(size_t)e] = fc.elems[(size_t)EToP[e]]++;
+  fc.pick.assign((size_t)P * P, {});
+  fc.place.assign((size_t)P * P, {});
+  const int64_t NF = (int64_t)Nfaces * Nfp;
+  for (int p = 0; p < P; ++p)  // partition p in ascending global element order
+    for (int64_t ge = 0; ge < K; ++ge) {
+      if (EToP[ge] != p) continue;
+      const int64_t le = local[(size_t)ge];
+      for (int64_t q = 0; q < NF; ++q) {
+        const int64_t src = vmapP[ge * NF + q];
+        if (src < 0 || src >= K * Np) throw std::invalid_argument("vmapP entry out of range");
+        const int64_t se = src / Np;
+        const int sp = (int)EToP[se];
+        fc.pick[(size_t)sp * P + p].push_back(local[(size_t)se] * Np + src % Np);
+        fc.place[(size_t)p * P + sp].push_back(le * NF + q);
+      }
+    }
+  // Verify: index validity, pick/place correspondence, conservation
+  int64_t total = 0;
+  for (int p = 0; p < P; ++p)
+    for (int q = 0; q < P; ++q) {
+      for (int64_t v : fc.pick[(size_t)p * P + q])
+        if (v < 0 || v >= fc.elems[p] * Np)
+          throw std::runtime_error("invalid pick index for partition " + std::to_string(p));
+      if (fc.pick[(size_t)p * P + q].size() != fc.place[(size_t)q * P + p].size())
+        throw std::runtime_error("pick/place length mismatch");
+      total += (int64_t)fc.pick[(size_t)p * P + q].size();
+    }
+  if (total != K * NF) throw std::runtime_error("conservation error: picks != face points");
+  return fc;
+}
+
+void face_gather_map(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmapP, const int64_t *EToP, int npart,
+                     const int64_t *node_off, int32_t *gmap) {
+  FaceConnector fc = face_connector(K, Nfaces, Nfp, Np, vmapP, EToP, npart);
+  const int P = fc.nparts;
+  const int64_t NF = (int64_t)Nfaces * Nfp;
+  std::vector<int64_t> face_base(P + 1, 0);  // P-buffers of all partitions back to back
+  for (int p = 0; p < P; ++p) face_base[p + 1] = face_base[p] + fc.elems[p] * NF;
+  for (int dst = 0; dst < P; ++dst)
+    for (int src = 0; src < P; ++src) {
+      const auto &pk = fc.pick[(size_t)src * P + dst];
+      const auto &pl = fc.place[(size_t)dst * P + src];
+      for (size_t i = 0; i < pk.size(); ++i) {
+        const int64_t v = node_off[src] + pk[i];
+        if (v > INT32_MAX) throw std::runtime_error("gather index exceeds int32");
+        gmap[face_base[dst] + pl[i]] = (int32_t)v;
+      }
+    }
+}
+
+uint64_t splitmix_next(uint64_t &state) {
+  state += 0x9E3779B97F4A7C15ull;
+  uint64_t z = state;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+double splitmix_uniform(uint64_t &state) { return (double)(splitmix_next(state) >> 11) * (1.0 / 9007199254740992.0); }
+
+}  // namespace dgk

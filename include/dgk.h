@@ -1,0 +1,188 @@
+/*
+ * dgk.h — C ABI of the B200 (sm_100a) backend for DGKernel's partition-parallel tet-DG right-hand side.
+ *
+ * The entry points replace the gocca/OCCA device layer under DGKernel's Go `runner` package for the
+ * named RHS kernels; every entry point cites the reference interface it stands in for (paths relative to
+ * the DGKernel project root).  All calls return an int status (DGK_OK = 0); the message of the last
+ * failure is available from dgk_last_error() (per runner) or dgk_global_error() (calls without a runner).
+ *
+ * Ownership: host pointers are used only for the duration of a call and never retained (cgo forbids C
+ * from keeping Go pointers).  Device memory is owned by the runner and released by dgk_runner_free.
+ * Threading: a runner is not thread-safe; all of its work is ordered on one CUDA stream.  Unlike the
+ * reference's ExecuteKernel, which calls Device.Finish() after every kernel
+ * (runner/kernel_execution.go:62), dgk_execute_kernel only synchronises when the configuration asks for
+ * a copy back; dgk_sync() is the explicit Finish.
+ */
+#ifndef DGK_H
+#define DGK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------------ */
+#define DGK_OK 0
+#define DGK_ERR_INVALID 1     /* bad argument; also the reference's panics (empty K, KpartMax > 2^20) */
+#define DGK_ERR_STATE 2       /* call out of order (define after allocate, execute before build, ...) */
+#define DGK_ERR_NOT_FOUND 3   /* unknown binding / kernel / op */
+#define DGK_ERR_CUDA 4        /* a CUDA runtime call failed */
+#define DGK_ERR_TIMEOUT 5     /* a device-side bounded wait gave up (status word set by the kernel) */
+#define DGK_ERR_UNSUPPORTED 6 /* valid request this backend does not implement */
+#define DGK_ERR_NO_DEVICE 7   /* no CUDA device: the backend has no CPU fallback */
+
+/* ---- enumerations mirroring runner/builder ------------------------------------------------------ */
+/* builder.DataType (runner/builder/builder.go:12-20) */
+#define DGK_FLOAT32 1
+#define DGK_FLOAT64 2
+#define DGK_INT32 3
+#define DGK_INT64 4
+/* builder.Direction (runner/builder/builder_param.go:10-17) */
+#define DGK_INPUT 0
+#define DGK_OUTPUT 1
+#define DGK_INOUT 2
+#define DGK_TEMP 3
+#define DGK_SCALAR 4
+/* runner.ActionFlags (runner/binding.go:15-26): CopyTo = 1<<1, CopyBack = 1<<2 */
+#define DGK_NO_ACTION 0
+#define DGK_COPY_TO 2
+#define DGK_COPY_BACK 4
+#define DGK_COPY 6
+/* host layout of an array binding: flat []T (element-contiguous already), or a row-major gonum
+ * mat.Matrix rows x cols that copies transpose to column-major (runner/kernel_copy.go:86-111) */
+#define DGK_LAYOUT_FLAT 0
+#define DGK_LAYOUT_MATRIX 1
+
+typedef struct dgk_runner dgk_runner;
+typedef struct dgk_element dgk_element;
+
+/* ---- runner lifecycle --------------------------------------------------------------------------- */
+/* NewRunner + builder.NewBuilder (runner/runner.go:48-86, runner/builder/builder.go:73-100).
+ * int_type is DGK_INT32 or DGK_INT64 (0 = INT64).  Fails with DGK_ERR_INVALID for npart < 1 or
+ * KpartMax > 2^20 (the reference panics), DGK_ERR_NO_DEVICE without a GPU. */
+int dgk_runner_create(const int64_t *K, int32_t npart, int32_t int_type, dgk_runner **out);
+/* A runner that plans without a device: bindings, aligned offsets, kernel signatures and the preamble
+ * work; copies, BuildKernel and ExecuteKernel fail with DGK_ERR_NO_DEVICE.  For host-side tooling. */
+int dgk_runner_create_host_only(const int64_t *K, int32_t npart, int32_t int_type, dgk_runner **out);
+/* Runner.Free (runner/runner.go:178-188). */
+int dgk_runner_free(dgk_runner *r);
+const char *dgk_last_error(const dgk_runner *r);
+const char *dgk_global_error(void);
+/* Use an existing cudaStream_t (as void*) for all work of this runner; NULL = the runner's own. */
+int dgk_set_stream(dgk_runner *r, void *cuda_stream);
+/* Device.Finish (runner/kernel_execution.go:62). */
+int dgk_sync(dgk_runner *r);
+
+/* ---- bindings (DefineBindings, runner/binding.go:100-195) --------------------------------------- */
+/* Array or temp binding.  part_values (part_count entries) gives the host values of each partition of a
+ * [][]T / []mat.Matrix binding; part_count 0 means non-partitioned.  A partitioned runner rejects
+ * non-partitioned arrays and a partition-count mismatch (binding.go:181-191).  layout/rows/cols describe
+ * a mat.Matrix host binding (rows x cols per partition for []mat.Matrix).  align is the
+ * builder.AlignmentType in bytes (0 or 1 = none). */
+int dgk_bind_array(dgk_runner *r, const char *name, int32_t dir, int32_t host_dtype, int32_t dev_dtype,
+                   int64_t total_values, int32_t part_count, const int64_t *part_values, int32_t align, int32_t layout,
+                   int64_t rows, int64_t cols);
+/* Input(name).Bind(mat).ToMatrix()[.Static()] (runner/binding.go:422-488).  Values row-major; stored on
+ * the device column-major (runner/runner.go:375-417).  dev_dtype FLOAT64/FLOAT32, or INT32 for integer
+ * tables such as Fmask. */
+int dgk_bind_matrix(dgk_runner *r, const char *name, int64_t rows, int64_t cols, const double *rowmajor,
+                    int32_t is_static, int32_t dev_dtype);
+/* Scalar(name)[.Bind(v)] (runner/builder/builder_param.go:86-95).  bound_value NULL = unbound. */
+int dgk_bind_scalar(dgk_runner *r, const char *name, int32_t dtype, const double *bound_value);
+/* AllocateDevice (runner/binding.go:339-384): one pooled device arena, aligned per-partition offsets
+ * (runner/builder/builder.go:113-159). */
+int dgk_allocate(dgk_runner *r);
+
+/* ---- copies (runner/memory_operations.go, runner/kernel_copy.go, runner/runner_copy.go) ----------- */
+/* CopyToDevice / CopyFromDevice of a whole binding (memory_operations.go:219-241).  The host buffer holds
+ * every partition back to back in the host type and layout; conversion f64<->f32 / i64<->i32 and the
+ * mat.Matrix transpose run on the GPU.  bytes must equal the binding's host size. */
+int dgk_copy_to_device(dgk_runner *r, const char *name, const void *host, int64_t bytes);
+int dgk_copy_from_device(dgk_runner *r, const char *name, void *host, int64_t bytes);
+/* One partition of a [][]T / []mat.Matrix binding (kernel_copy.go:288-560), the cgo-safe form. */
+int dgk_copy_partition_to_device(dgk_runner *r, const char *name, int32_t part, const void *host, int64_t bytes);
+int dgk_copy_partition_from_device(dgk_runner *r, const char *name, int32_t part, void *host, int64_t bytes);
+/* Host-side copy of `<name>_offsets` (runner/runner.go:227-254), npart+1 values. */
+int dgk_get_offsets(dgk_runner *r, const char *name, int64_t *out);
+/* Device address of `<name>_global` (or of a matrix), for zero-copy interop. */
+int dgk_device_ptr(dgk_runner *r, const char *name, void **out);
+
+/* ---- kernels (runner/kernel_config.go, runner/kernel_execution.go, runner/runner.go:88-126) ------- */
+/* ConfigureKernel(name, Param(p).CopyTo()...) (kernel_config.go:51-91). */
+int dgk_configure_kernel(dgk_runner *r, const char *kname, int32_t nparams, const char *const *params,
+                         const uint32_t *actions);
+/* BuildKernel(src, name) (runner/runner.go:88-126): selects the precompiled sm_100a operator `op_id`
+ * ("differentiate", "computeRHS", "updateSolution", "rhsStage", "rhsLF", "lserkUpdate", "matmul",
+ * "matmulAdd", "faceGather") instead of JIT-compiling OKL.  Operator roles bind to configured parameters
+ * by name; `op_id` may carry explicit role=binding pairs, e.g. "matmul(M=Dr_NudgTet2,IN=U,OUT=Ur)". */
+int dgk_build_kernel(dgk_runner *r, const char *kname, const char *op_id);
+/* ExecuteKernel(name, scalars...) (kernel_execution.go:12-89): pre-copies (CopyTo), launch, post-copies
+ * (CopyBack).  host_ptrs[i] is the host buffer of configured parameter i (NULL = no copy).  Scalars are
+ * resolved as the reference does: a bound value first, then the positional list (kernel_execution.go:
+ * 114-138). */
+int dgk_execute_kernel(dgk_runner *r, const char *kname, int32_t nscalars, const double *scalars,
+                       void *const *host_ptrs);
+/* GetKernelSignatureForConfig (kernel_execution.go:230-237, kernel_config.go:183-246): OKL argument list. */
+int dgk_kernel_signature(dgk_runner *r, const char *kname, char *buf, int64_t buflen);
+/* GeneratePreamble (runner/builder/builder.go:172-410): the text the reference prepends to OKL. */
+int dgk_generate_preamble(dgk_runner *r, char *buf, int64_t buflen);
+
+/* ---- reference element (element/library/gonudg: startup3d.go, lift3d.go, nodes3d.go) -------------- */
+/* NewDG3D's mesh-independent operators for order N (1..8), FP64 on the host. */
+int dgk_element_create(int32_t N, dgk_element **out);
+int dgk_element_free(dgk_element *e);
+int dgk_element_dims(const dgk_element *e, int32_t *Np, int32_t *Nfp);
+/* Row-major copy of "r","s","t" (Np), "V","Vinv","MassMatrix","M","Minv","Dr","Ds","Dt" (Np x Np) or
+ * "LIFT" (Np x 4Nfp); names as GetRefMatrices (tetnudg/tet_nudg_mesh.go:371-389). */
+int dgk_element_get(const dgk_element *e, const char *what, double *out, int64_t count);
+/* Fmask, 4 x Nfp (startup3d.go:179-209). */
+int dgk_element_fmask(const dgk_element *e, int32_t *out);
+
+/* ---- mesh, connectivity and face maps ------------------------------------------------------------ */
+/* Structured n^3 Kuhn-cube mesh on [lo,hi]^3 (6 tets per cube, utils/mesh_test_helpers.go:346-388
+ * order), cubes x-slowest, EToP = x-slab of nslab slabs.  VX/VY/VZ: (n+1)^3; EToV, EToV_periodic
+ * (vertex ids wrapped mod n for periodic face matching) and EToP: 6n^3 entries (EToV 4 per element). */
+int dgk_kuhn_mesh(int32_t n, int32_t nslab, double lo, double hi, double *VX, double *VY, double *VZ,
+                  int64_t *EToV, int64_t *EToV_periodic, int64_t *EToP);
+/* tiConnect3D (element/library/gonudg/ticonnect3d.go:24-102). */
+int dgk_ti_connect3d(int64_t K, const int64_t *EToV, int64_t *EToE, int64_t *EToF);
+/* FaceConnector (utils/face_connector.go:43-187).  First call with pick_idx == NULL to get the
+ * (npart*npart) list lengths in pick_len (pick_len[src*npart+dst] == place_len[dst*npart+src]); then
+ * call again with pick_idx/place_idx sized to the sums to receive the lists, CSR-concatenated in pair
+ * order.  Verify (face_connector.go:208-253) runs on every build. */
+int dgk_face_connector(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP,
+                       const int64_t *EToP, int32_t npart, int64_t *pick_len, int64_t *pick_idx,
+                       int64_t *place_idx);
+/* Fused pick->exchange->place gather map: for every face point of partition p (in that partition's
+ * P-buffer order), the absolute value index of its neighbour node in an array whose partition p starts
+ * at node_off[p].  This is the one-address-space form of the FaceConnector exchange. */
+int dgk_face_gather_map(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP,
+                        const int64_t *EToP, int32_t npart, const int64_t *node_off, int32_t *gmap);
+
+/* GPU FP64 setup (element/library/gonudg/startup3d.go:121-148, normals3d.go:11-207,
+ * buildmaps3d.go:5-153) into the runner's bound arrays.  names[] lists the target binding for each of
+ * "X","Y","Z","Rx","Ry","Rz","Sx","Sy","Sz","Tx","Ty","Tz","J","nx","ny","nz","sJ","Fscale","vmapM",
+ * "vmapP" (20 entries; NULL = skip).  Node arrays hold Np values and face arrays 4*Nfp values per
+ * element; partitions are the contiguous element ranges of the runner's K.  period: 0 = no periodic
+ * matching, else the box length used to wrap coordinate differences.  EToE/EToF as tiConnect3D.
+ * hmin_out (may be NULL) receives the smallest node-pair distance
+ * (examples/3d_scalar_burgers_equation.go:697-717).  vmapM/vmapP targets may be int32 or int64. */
+int dgk_setup_geometry(dgk_runner *r, const dgk_element *e, int64_t nverts, const double *VX, const double *VY,
+                       const double *VZ, const int64_t *EToV, const int64_t *EToE, const int64_t *EToF,
+                       double period, const char *const *names, double *hmin_out);
+
+/* ---- seeded synthetic inputs --------------------------------------------------------------------- */
+/* Evaluate an initial field at the node coordinates bound as xname/yname/zname (same type and layout):
+ * kind 0: mean + amp sin(pi x) sin(pi y) sin(pi z); kind 1: mean + amp sin(pi x) cos(pi y) sin(pi z);
+ * kind 2: mean + sum_m a_m cos(pi (k_m . x) + phi_m) with modes rows (kx, ky, kz, a, phi). */
+int dgk_init_field(dgk_runner *r, const char *name, const char *xname, const char *yname, const char *zname,
+                   int32_t kind, double mean, double amp, int32_t nmodes, const double *modes);
+/* splitmix64 uniform stream (53-bit doubles), for reproducible inputs across host and oracle. */
+int dgk_splitmix_uniform(uint64_t seed, int64_t count, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DGK_H */

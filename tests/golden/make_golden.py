@@ -1,0 +1,89 @@
+"""Extract the reference's own golden vectors and in-code test meshes into tests/golden/reference_golden.json.
+
+Run once in a checkout that has the DGKernel sources (default /root/reference, or DGK_REFERENCE_ROOT); the
+JSON it writes is committed, so the tests never read the reference at run time.  It reads the reference's
+Go test files as text:
+
+  * element/library/gonudg/jacobi_quadrature_test.go  TestJacobiGL table (alpha, beta, N, expected nodes)
+  * element/library/gonudg/jacobip_test.go            P_0^(a,0) values and the P_{0,0,0} product
+  * utils/mesh_test_helpers.go                        createCubeNodes / createCubeMesh / createTwoTetMesh
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import re
+import sys
+
+ROOT = os.environ.get("DGK_REFERENCE_ROOT", "/root/reference")
+OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
+
+
+def _go_expr(expr: str) -> float:
+    expr = expr.replace("math.Sqrt", "math.sqrt").replace("math.Pi", "math.pi")
+    return float(eval(expr, {"math": math, "__builtins__": {}}))
+
+
+def jacobi_gl_table(text: str):
+    body = text[text.index("func TestJacobiGL("):text.index("func TestJacobiGQ(")]
+    cases = []
+    for m in re.finditer(r"\{\s*name:\s*\"([^\"]+)\",(.*?)\n\t\t\},", body, re.S):
+        blk = m.group(2)
+        alpha = float(re.search(r"alpha:\s*([-\d.]+)", blk).group(1))
+        beta = float(re.search(r"beta:\s*([-\d.]+)", blk).group(1))
+        n = int(re.search(r"\bN:\s*(\d+)", blk).group(1))
+        exp = re.search(r"expected:\s*\[\]float64\{(.*?)\}", blk, re.S).group(1)
+        vals = [float(v) for v in re.findall(r"[-+]?\d*\.?\d+(?:e[-+]?\d+)?", exp)]
+        tol = float(re.search(r"tol:\s*([-\d.e]+)", blk).group(1))
+        cases.append({"name": m.group(1), "alpha": alpha, "beta": beta, "N": n, "expected": vals, "tol": tol})
+    return cases
+
+
+def jacobi_p_values(text: str):
+    vals = []
+    for m in re.finditer(r"(\w+)\s*:=\s*JacobiP\(x,\s*([-\d.]+),\s*([-\d.]+),\s*(\d+)\)\s*\n\s*(\w+)\s*:=\s*([^\n]+)",
+                         text):
+        vals.append({"alpha": float(m.group(2)), "beta": float(m.group(3)), "N": int(m.group(4)),
+                     "x": [-1.0, 0.0, 1.0], "value": _go_expr(m.group(6).split("//")[0].strip()), "tol": 1e-14})
+    return vals
+
+
+def meshes(text: str):
+    nodes_blk = re.search(r"func createCubeNodes\(\) NodeSet \{(.*?)\n\}", text, re.S).group(1)
+    coords = [[float(v) for v in row.split(",")] for row in re.findall(r"\{([-\d., ]+)\},\s*//", nodes_blk)]
+    names = dict((k, int(v)) for k, v in re.findall(r"\"(\w+)\":\s*(\d+)", nodes_blk))
+    cube_blk = re.search(r"func createCubeMesh\(\) CompleteMesh \{(.*?)\n\}", text, re.S).group(1)
+    cube = [[names[n] for n in re.findall(r"\"(\w+)\"", row)] for row in re.findall(r"\{(\"[^}]*)\}", cube_blk)]
+    two_blk = re.search(r"func createTwoTetMesh\(\) CompleteMesh \{(.*?)\n\}", text, re.S).group(1)
+    node_part = two_blk[two_blk.index("Nodes: [][]float64{"):two_blk.index("NodeMap")]
+    two_nodes = [[float(v) for v in row.split(",")] for row in re.findall(r"\{([-\d., ]+)\},", node_part)]
+    two_names = dict((k, int(v)) for k, v in re.findall(r"\"(v\d)\":\s*(\d+)", two_blk))
+    two = [[two_names[n] for n in re.findall(r"\"(v\d)\"", row)]
+           for row in re.findall(r"\{(\"v\d\",[^}]*)\}", two_blk)]
+    return {"cube_nodes": coords[:8], "cube_tets": [t for t in cube if len(t) == 4],
+            "two_tet_nodes": two_nodes, "two_tet_tets": two}
+
+
+def main():
+    g = os.path.join(ROOT, "element", "library", "gonudg")
+    with open(os.path.join(g, "jacobi_quadrature_test.go")) as f:
+        quad = f.read()
+    with open(os.path.join(g, "jacobip_test.go")) as f:
+        jp = f.read()
+    with open(os.path.join(ROOT, "utils", "mesh_test_helpers.go")) as f:
+        helpers = f.read()
+    out = {
+        "source": "DGKernel test files read as text by tests/golden/make_golden.py",
+        "jacobi_gl": jacobi_gl_table(quad),
+        "jacobi_p": jacobi_p_values(jp),
+        "simplex3dp_000": math.sqrt(3.0) / 2.0,
+        "meshes": meshes(helpers),
+    }
+    with open(OUT, "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {OUT}: {len(out['jacobi_gl'])} JacobiGL cases, {len(out['jacobi_p'])} JacobiP values")
+
+
+if __name__ == "__main__":
+    sys.exit(main())
