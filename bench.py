@@ -1,0 +1,310 @@
+"""Benchmark of the tet-DG RHS hot path on B200: DOF-stage-updates/s of LSERK4 stages.
+
+Workload: 3-D scalar Burgers, nodal DG order N=4 (Np=35, Nfp=15) on a periodic 64^3 x 6
+Kuhn-cube mesh (K = 1,572,864 tets), 16 x-slab partitions, u0 = 0.5 + 8 seeded random Fourier modes.  One
+"step" is one LSERK4 stage over all K elements: the fused volume + Lax-Friedrichs surface + LIFT + stage update
+kernel.  The plain FP64 form and the FP32 form run from the same initial state; `value` is the chosen form
+(the faster one whose L2 error against the FP64 run stays <= 1e-6 after the timed stages).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 64] [--order 4]
+Under torchrun (N > 1) every rank runs an independent replica (the path shards by partition; one GPU per
+replica) and the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "DOF-stage-updates/s on 1 B200, chosen vs plain FP64 at L2 err≤1e-6; %HBM"
+UNIT = "DOF-stage-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def b_alg_per_dof(N: int, elem_bytes: int) -> float:
+    """Algorithmic bytes per DOF-stage of the fused stage kernel in the reference-contract layout:
+    u read + resu read + resu write + u write, 9 per-node metrics, and per face point nx, ny, nz, Fscale plus
+    one int32 gather index, spread over the Np nodes (neighbour traces assumed L2 hits)."""
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    Nfp = (N + 1) * (N + 2) // 2
+    r = 4 * Nfp / Np
+    return 4 * elem_bytes + 9 * elem_bytes + r * (4 * elem_bytes + 4)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 100 ms while running."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def time_stages(prob, steps: int, stream):
+    """Run `steps` stages on `stream`, CUDA events on that stream, synchronize on both sides."""
+    import torch
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    prob.run_stages(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps  # ms per stage
+
+
+def cpu_baseline(N: int, steps: int, seconds: float = 12.0):
+    """Oracle port (C restatement of the OKL loops, OpenMP over the @outer partition loop) on a bounded
+    sample of the same workload: order N, 16 x-slab partitions of a 16^3 x 6 Kuhn mesh (24,576 tets)."""
+    from oracle import oracle as O
+    from dgkernel_b200.burgers import BurgersProblem, GEO, FACE
+    from dgkernel_b200 import mesh as M
+    prob = BurgersProblem(N, 16, 16, np.float64, "modes")
+    el = prob.el
+    geo = [prob.get(nm) for nm in GEO]
+    face = [prob.get(nm) for nm in FACE]
+    fc = M.FaceConnector(prob.K, 4, el.Nfp, el.Np, prob.vmapP, prob.EToP)
+    P = fc.NumPartitions
+    pick_ptr, pick_idx = O.csr_pairs(fc.pick, P)
+    place_ptr, place_idx = O.csr_pairs(fc.place, P)
+    K = np.asarray(prob.Kpart, dtype=np.int64)
+    noff = np.concatenate(([0], np.cumsum(K * el.Np))).astype(np.int64)
+    foff = np.concatenate(([0], np.cumsum(K * 4 * el.Nfp))).astype(np.int64)
+    mats = [O.cm(el.Dr), O.cm(el.Ds), O.cm(el.Dt), O.cm(el.LIFT)]
+    fmask = np.ascontiguousarray(el.Fmask.reshape(-1).astype(np.int32))
+    u = np.ascontiguousarray(prob.u0.astype(np.float64))
+    resu = np.zeros_like(u)
+    dt = prob.dt
+    prob.free()
+    threads = max(1, min(os.cpu_count() or 1, P))
+    L = O.lib()
+    args = (el.Np, el.Nfp, *mats, fmask, P, K, noff, foff, u, resu, *geo, *face, pick_ptr, pick_idx, place_ptr,
+            place_idx, float(dt))
+    L.ora_run(*args, 0, 1, 0, threads)  # warm-up stage
+    done, t0 = 0, time.perf_counter()
+    while True:
+        L.ora_run(*args, done % 5, 1, 0, threads)
+        done += 1
+        el_t = time.perf_counter() - t0
+        if (steps and done >= steps) or (not steps and el_t >= seconds):
+            break
+    value = prob.dofs * done / el_t
+    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"order {N}, 16^3x6 Kuhn mesh (24,576 tets, {P} x-slab partitions), {done} LSERK4 stages of "
+                      f"exchange + LF RHS + update, C restatement of the OKL loops (gcc -O3 -fopenmp, "
+                      f"-ffp-contract=off), OpenMP over partitions, {threads} threads of {os.cpu_count()} host cores",
+            "seconds": el_t}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    base = cpu_baseline(args.order, args.steps)
+    out = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": base["seconds"] / max(1, args.steps) * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": f"3-D Burgers tet-DG LSERK4 stage, order {args.order}, sampled on a 16^3x6 "
+                                  f"periodic Kuhn mesh with 16 x-slab partitions (the reference's CPU path)"},
+           "cpu_baseline": base, "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--order", type=int, default=4)
+    ap.add_argument("--slabs", type=int, default=16)
+    ap.add_argument("--e2e-steps", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+
+    import torch
+    from dgkernel_b200.burgers import BurgersProblem, RK4A, RK4B
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    hbm, peak_kind = peaks()
+    results = {}
+    finals = {}
+    for name, dt in (("f64", np.float64), ("f32", np.float32)):
+        prob = BurgersProblem(args.order, args.n, args.slabs, dt, "modes", stream=stream.cuda_stream)
+        prob.run_stages(args.warmup)
+        barrier(world)
+        with ClockSampler(local) as clk:
+            ms = time_stages(prob, args.steps, stream)
+        ms = max_over_ranks(ms, world)
+        finals[name] = prob.get("u").astype(np.float64)
+        results[name] = {"ms": ms, "dofs": prob.dofs, "clocks": clk.summary(), "prob": prob,
+                         "elem_bytes": 8 if dt == np.float64 else 4}
+        if name == "f32":
+            prob.free()
+    err = float(np.linalg.norm(finals["f32"] - finals["f64"]) / np.linalg.norm(finals["f64"]))
+    dofs = results["f64"]["dofs"]
+    thr = {k: world * dofs / (v["ms"] * 1e-3) for k, v in results.items()}
+    chosen = "f32" if (err <= 1e-6 and thr["f32"] > thr["f64"]) else "f64"
+    ch = results[chosen]
+
+    # end to end through the runner's ExecuteKernel: H2D of u and resu from pinned host memory, the stage, D2H of
+    # u and resu (the copy pattern of examples/3d_scalar_burgers_equation.go:269-270), FP64 path
+    prob = results["f64"]["prob"]
+    r = prob.runner
+    sn = prob.el.ShortName
+    from dgkernel_b200.burgers import GEO, FACE
+    hu = torch.empty(dofs, dtype=torch.float64, pin_memory=True).numpy()
+    hr = torch.empty(dofs, dtype=torch.float64, pin_memory=True).numpy()
+    r.CopyFromDevice("u", hu)
+    r.CopyFromDevice("resu", hr)
+    r.Bindings["u"].host, r.Bindings["resu"].host = hu, hr
+    fixed = ["u", "uNext", "resu", *GEO, *FACE, "gmap", f"Dr_{sn}", f"Ds_{sn}", f"Dt_{sn}", f"LIFT_{sn}", "Fmask"]
+    params = [r.Param(p).Copy() if p in ("u", "resu") else r.Param(p) for p in fixed]
+    r.ConfigureKernel("stageE2E", *params, r.Param("a"), r.Param("b"), r.Param("dt"))
+    r.BuildKernel("rhsStage", "stageE2E")
+    r.ExecuteKernel("stageE2E", RK4A[0], RK4B[0], prob.dt)
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in range(args.e2e_steps):
+        r.ExecuteKernel("stageE2E", RK4A[s % 5], RK4B[s % 5], prob.dt)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.e2e_steps, world)
+    prob.free()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args.order, 0)
+    if rank == 0:
+        bpd = b_alg_per_dof(args.order, ch["elem_bytes"])
+        achieved = bpd * dofs / (ch["ms"] * 1e-3) / 1e9
+        traffic = None
+        try:
+            with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+                tj = json.load(f)
+            key = f"rhs_stage_N{args.order}_{chosen}"
+            if key in tj:
+                traffic = tj[key]["dram_bytes_per_dof"] * dofs
+        except Exception:
+            pass
+        out = {
+            "metric": METRIC, "value": thr[chosen], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ch["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": chosen, "data": "synthetic",
+            "config": {"workload": f"3-D Burgers tet-DG, order {args.order} (Np={(args.order+1)*(args.order+2)*(args.order+3)//6}), "
+                                   f"periodic {args.n}^3x6 Kuhn mesh (K={dofs // ((args.order+1)*(args.order+2)*(args.order+3)//6)}), "
+                                   f"{args.slabs} x-slab partitions, u0 = 0.5 + 8 seeded Fourier modes; one step = one "
+                                   f"LSERK4 stage", "form": "plain", "chosen": chosen,
+                       "l2": "inputs larger than L2 (every stage streams GBs of state, metrics and face data)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+            "chosen_vs_plain_fp64": {"fp64": thr["f64"], "fp32": thr["f32"], "fp32_l2_err_vs_fp64": err,
+                                     "speedup": thr[chosen] / thr["f64"]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                         "b_alg_per_dof": bpd, "kernel": "rhs_stage_kernel"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * dofs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * dofs * 8,
+                    "d2h_bytes_per_step": 2 * dofs * 8, "path": "Runner.ExecuteKernel (C ABI) with Copy() of u, resu"},
+            "clocks": ch["clocks"],
+            "gpu_launches": args.steps,
+        }
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

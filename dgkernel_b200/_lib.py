@@ -31,6 +31,7 @@ SIGNATURES = {
     "dgk_copy_from_device": [_P, _S, _P, _I64],
     "dgk_copy_partition_to_device": [_P, _S, _I32, _P, _I64],
     "dgk_copy_partition_from_device": [_P, _S, _I32, _P, _I64],
+    "dgk_copy_raw_from_device": [_P, _S, _I64, _P, _I64],
     "dgk_get_offsets": [_P, _S, _PI64],
     "dgk_device_ptr": [_P, _S, C.POINTER(_P)],
     "dgk_configure_kernel": [_P, _S, _I32, C.POINTER(_S), C.POINTER(C.c_uint32)],

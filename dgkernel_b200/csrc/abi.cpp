@@ -107,6 +107,21 @@ int dgk_copy_partition_to_device(dgk_runner *r, const char *name, int32_t part, 
 int dgk_copy_partition_from_device(dgk_runner *r, const char *name, int32_t part, void *host, int64_t bytes) {
   return guard(r, [&] { r->impl.copy_partition_from_device(name, part, host, bytes); });
 }
+int dgk_copy_raw_from_device(dgk_runner *r, const char *name, int64_t value_offset, void *host, int64_t bytes) {
+  return guard(r, [&] {
+    dgk::Runner &R = r->impl;
+    R.need_device("dgk_copy_raw_from_device");
+    dgk::Binding &b = R.binding(name);
+    if (b.is_scalar) throw dgk::Error(DGK_ERR_INVALID, b.name + " is a scalar");
+    const int64_t es = dgk::dtype_size(b.dev_dtype);
+    if (value_offset < 0 || bytes < 0 || (size_t)(value_offset * es + bytes) > b.dbytes)
+      throw dgk::Error(DGK_ERR_INVALID, "raw read outside " + b.name);
+    dgk::cuda_check(cudaMemcpyAsync(host, b.dptr + value_offset * es, (size_t)bytes, cudaMemcpyDeviceToHost,
+                                    R.stream()), "D2H raw copy");
+    dgk::cuda_check(cudaStreamSynchronize(R.stream()), "sync");
+  });
+}
+
 int dgk_get_offsets(dgk_runner *r, const char *name, int64_t *out) {
   return guard(r, [&] {
     dgk::Binding &b = r->impl.binding(name);

@@ -27,6 +27,9 @@ struct Tile {
 // Status word codes written by kernels (never a trap: the host reads the word and reports).
 enum : int { kStatusOk = 0, kStatusBadGather = 1 };
 
+// Even row stride of matrices as the kernels read them (pairs of entries load as one vector).
+constexpr int pad_even(int c) { return (c + 1) & ~1; }
+
 template <int N>
 struct Order {
   static constexpr int NP = (N + 1) * (N + 2) * (N + 3) / 6;
@@ -68,8 +71,8 @@ struct RhsArgs {
   const T *face[4];      // nx, ny, nz, Fscale per face point
   const int32_t *gmap;   // neighbour value index per face point (fused FaceConnector exchange)
   int64_t n_u_values;    // bound of gmap entries
-  const T *Dmat;         // [3][NP][NP] Dr, Ds, Dt
-  const T *LIFT;         // [NP][NF]
+  const T *Dmat;         // [3][NP][pad(NP)] Dr, Ds, Dt; rows padded to an even length (16-byte pairs)
+  const T *LIFT;         // [NP][pad(NF)]
   const int32_t *fmask;  // [NF]
   T a, b, dt;            // LSERK stage coefficients
   int conservative;      // 0: -u (ux+uy+uz) (reference form), 1: -div(u^2/2 (1,1,1))
@@ -84,7 +87,7 @@ struct DiffArgs {
   const T *geo[9];
   T *out[3];   // differentiate: DuDx, DuDy, DuDz;  computeRHS: out[0] = rhsu
   int mode;    // 0 = differentiate, 1 = reference volume-only computeRHS
-  const T *Dmat;
+  const T *Dmat;  // [3][NP][pad(NP)], rows padded to an even length
 };
 
 }  // namespace dgk

@@ -1,6 +1,7 @@
 // sm_100a kernels: type conversion for the copy engine, and the tet-DG hot path (volume derivative,
 // reference-form computeRHS / updateSolution, fused Lax-Friedrichs RHS + LSERK4 stage).
 #include <cstdint>
+#include <type_traits>
 
 #include "dg_kernels.cuh"
 #include "kernels.hpp"
@@ -94,26 +95,74 @@ __device__ __forceinline__ T lds(const T *p) { return __ldcs(p); }
 template <typename T>
 __device__ __forceinline__ void sts(T *p, T v) { __stcs(p, v); }
 
-// Three stacked NP x NP matrices times the element vectors of a shared-memory tile, for the RG rows of row
-// group g: acc[m][r] = sum_j M[m][g*RG + r][j] * f(x[e][j]), f(x) = x or x^2/2.
-template <typename T, int NP, int RG, int NM, bool SQUARE>
+// Bulk prefetch of a contiguous global range into L2 (TMA, no shared memory involved).  The range is widened
+// to 16-byte granules; every array lives in a 256-byte aligned slot of the runner's arena, so the widened
+// range stays inside the array's slot.
+__device__ __forceinline__ void prefetch_l2(const void *p, size_t bytes) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p) & ~uintptr_t(15);
+  const uintptr_t e = (reinterpret_cast<uintptr_t>(p) + bytes + 15) & ~uintptr_t(15);
+  if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((unsigned)(e - a)) : "memory");
+}
+
+// Row stride of a matrix staged in shared memory: even, so (j, j+1) pairs load as one 16-byte vector.
+template <int C>
+struct Pad {
+  static constexpr int V = (C + 1) & ~1;
+};
+
+// NM stacked NR x NC matrices (row stride Pad<NC>::V) times one element vector of a shared-memory tile, for
+// the RG rows of row group g: acc[m][r] = sum_j M[m][g*RG + r][j] * f(x[j]), f(x) = x or x^2/2.  The j loop
+// walks column pairs so each matrix entry pair is one 128-bit broadcast load.
+template <typename T, int NR, int NC, int RG, int NM, bool SQUARE>
 __device__ __forceinline__ void rows_matvec(const T *__restrict__ M, const T *xe, int g, T (&acc)[NM][RG]) {
+  constexpr int LD = Pad<NC>::V;
+  using T2 = typename std::conditional<sizeof(T) == 8, double2, float2>::type;
 #pragma unroll
   for (int m = 0; m < NM; ++m)
 #pragma unroll
     for (int r = 0; r < RG; ++r) acc[m][r] = T(0);
   const int i0 = g * RG;
-#pragma unroll 4
-  for (int j = 0; j < NP; ++j) {
-    T xj = xe[j];
-    if (SQUARE) xj = T(0.5) * xj * xj;
+#pragma unroll 2
+  for (int j = 0; j + 1 < NC; j += 2) {
+    T x0 = xe[j], x1 = xe[j + 1];
+    if (SQUARE) {
+      x0 = T(0.5) * x0 * x0;
+      x1 = T(0.5) * x1 * x1;
+    }
 #pragma unroll
     for (int r = 0; r < RG; ++r) {
-      const int i = min(i0 + r, NP - 1);  // rows past NP compute a duplicate that is never stored
+      const int i = min(i0 + r, NR - 1);  // rows past NR compute a duplicate that is never stored
 #pragma unroll
-      for (int m = 0; m < NM; ++m) acc[m][r] = fma(M[(m * NP + i) * NP + j], xj, acc[m][r]);
+      for (int m = 0; m < NM; ++m) {
+        const T2 mm = *reinterpret_cast<const T2 *>(M + (m * NR + i) * LD + j);
+        acc[m][r] = fma(mm.x, x0, acc[m][r]);
+        acc[m][r] = fma(mm.y, x1, acc[m][r]);
+      }
     }
   }
+  if (NC & 1) {
+    T x0 = xe[NC - 1];
+    if (SQUARE) x0 = T(0.5) * x0 * x0;
+#pragma unroll
+    for (int r = 0; r < RG; ++r) {
+      const int i = min(i0 + r, NR - 1);
+#pragma unroll
+      for (int m = 0; m < NM; ++m) acc[m][r] = fma(M[(m * NR + i) * LD + NC - 1], x0, acc[m][r]);
+    }
+  }
+}
+
+// Issue L2 prefetches for every stream a tile of the fused stage reads.
+template <typename T>
+__device__ __forceinline__ void prefetch_tile(const RhsArgs<T> &A, const Tile &tl, int np, int nf) {
+  const size_t nn = (size_t)tl.nelem * np, fn = (size_t)tl.nelem * nf;
+  prefetch_l2(A.u_in + tl.node_base, nn * sizeof(T));
+  if (A.resu) prefetch_l2(A.resu + tl.node_base, nn * sizeof(T));
+#pragma unroll
+  for (int k = 0; k < 9; ++k) prefetch_l2(A.geo[k] + tl.node_base, nn * sizeof(T));
+#pragma unroll
+  for (int k = 0; k < 4; ++k) prefetch_l2(A.face[k] + tl.face_base, fn * sizeof(T));
+  prefetch_l2(A.gmap + tl.face_base, fn * sizeof(int32_t));
 }
 
 // Shared-memory carve-up of the fused kernels.
@@ -121,8 +170,8 @@ template <typename T, int N, bool MSMEM>
 struct Smem {
   using O = Order<N>;
   using C = Cfg<N>;
-  static constexpr int DM = MSMEM ? 3 * O::NP * O::NP : 0;
-  static constexpr int LM = MSMEM ? O::NP * O::NF : 0;
+  static constexpr int DM = MSMEM ? 3 * O::NP * Pad<O::NP>::V : 0;
+  static constexpr int LM = MSMEM ? O::NP * Pad<O::NF>::V : 0;
   static constexpr int U = C::TE * O::NPS;
   static constexpr int D3 = 3 * C::TE * O::NPS;
   static constexpr int F = C::TE * O::NFS;
@@ -143,9 +192,10 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
   T *sf = sd + S::D3;
   int *sfm = reinterpret_cast<int *>(sf + S::F);
   const int tid = threadIdx.x, nth = blockDim.x;
-  if (MSMEM) {
-    for (int i = tid; i < 3 * NP * NP; i += nth) sD[i] = A.Dmat[i];
-    for (int i = tid; i < NP * NF; i += nth) sL[i] = A.LIFT[i];
+  if (tid == 0 && blockIdx.x < A.ntiles) prefetch_tile(A, A.tiles[blockIdx.x], NP, NF);
+  if (MSMEM) {  // the operator stores both matrices with the padded row strides used here
+    for (int i = tid; i < S::DM; i += nth) sD[i] = A.Dmat[i];
+    for (int i = tid; i < S::LM; i += nth) sL[i] = A.LIFT[i];
   }
   for (int i = tid; i < NF; i += nth) sfm[i] = A.fmask[i];
   const T *Dm = MSMEM ? sD : A.Dmat;
@@ -156,6 +206,7 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
 
   for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
     const Tile tl = A.tiles[t];
+    if (tid == 0 && t + (int)gridDim.x < A.ntiles) prefetch_tile(A, A.tiles[t + gridDim.x], NP, NF);
     const int ne = tl.nelem;
     const T *ug = A.u_in + tl.node_base;
     // P0: the tile's state, coalesced
@@ -168,9 +219,9 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
     if (e_own < ne) {
       T acc[3][RG];
       if (A.conservative)
-        rows_matvec<T, NP, RG, 3, true>(Dm, su + e_own * NPS, g_own, acc);
+        rows_matvec<T, NP, NP, RG, 3, true>(Dm, su + e_own * NPS, g_own, acc);
       else
-        rows_matvec<T, NP, RG, 3, false>(Dm, su + e_own * NPS, g_own, acc);
+        rows_matvec<T, NP, NP, RG, 3, false>(Dm, su + e_own * NPS, g_own, acc);
 #pragma unroll
       for (int r = 0; r < RG; ++r) {
         const int i = g_own * RG + r;
@@ -214,22 +265,10 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
     // P3: rhs = volume + LIFT * (Fscale du)
     if (e_own < ne) {
       T acc[1][RG];
-#pragma unroll
-      for (int r = 0; r < RG; ++r) acc[0][r] = T(0);
-      const T *fe = sf + e_own * NFS;
-      const int i0 = g_own * RG;
-#pragma unroll 4
-      for (int j = 0; j < NF; ++j) {
-        const T fj = fe[j];
-#pragma unroll
-        for (int r = 0; r < RG; ++r) {
-          const int i = min(i0 + r, NP - 1);
-          acc[0][r] = fma(Lm[i * NF + j], fj, acc[0][r]);
-        }
-      }
+      rows_matvec<T, NP, NF, RG, 1, false>(Lm, sf + e_own * NFS, g_own, acc);
 #pragma unroll
       for (int r = 0; r < RG; ++r) {
-        const int i = i0 + r;
+        const int i = g_own * RG + r;
         if (i < NP) sd[e_own * NPS + i] += acc[0][r];
       }
     }
@@ -259,11 +298,11 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) diff_kernel(DiffArgs<T> A) {
   constexpr int NP = O::NP, NPS = O::NPS, TE = C::TE, RG = C::RG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sD = reinterpret_cast<T *>(smem_raw);
-  T *su = sD + (MSMEM ? 3 * NP * NP : 0);
+  T *su = sD + (MSMEM ? 3 * NP * Pad<NP>::V : 0);
   T *sd = su + TE * NPS;
   const int tid = threadIdx.x, nth = blockDim.x;
   if (MSMEM)
-    for (int i = tid; i < 3 * NP * NP; i += nth) sD[i] = A.Dmat[i];
+    for (int i = tid; i < 3 * NP * Pad<NP>::V; i += nth) sD[i] = A.Dmat[i];
   const T *Dm = MSMEM ? sD : A.Dmat;
   const int e_own = tid % TE, g_own = tid / TE;
   __syncthreads();
@@ -277,7 +316,7 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) diff_kernel(DiffArgs<T> A) {
     __syncthreads();
     if (e_own < ne) {
       T acc[3][RG];
-      rows_matvec<T, NP, RG, 3, false>(Dm, su + e_own * NPS, g_own, acc);
+      rows_matvec<T, NP, NP, RG, 3, false>(Dm, su + e_own * NPS, g_own, acc);
 #pragma unroll
       for (int r = 0; r < RG; ++r) {
         const int i = g_own * RG + r;
@@ -387,7 +426,7 @@ static void diff_launch_n(const DiffArgs<T> &A, int num_sms, cudaStream_t st, La
   using C = Cfg<N>;
   const int threads = C::THREADS;
   const size_t base = sizeof(T) * (size_t)(4 * C::TE * O::NPS);
-  const size_t with = base + sizeof(T) * 3 * O::NP * O::NP;
+  const size_t with = base + sizeof(T) * 3 * O::NP * Pad<O::NP>::V;
   if (with <= 160 * 1024) {
     auto k = diff_kernel<T, N, true>;
     const int per = std::max(1, resident(k, threads, with));

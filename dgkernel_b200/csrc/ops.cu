@@ -107,6 +107,18 @@ std::vector<T> cast(const std::vector<double> &v) {
   return std::vector<T>(v.begin(), v.end());
 }
 
+// Row-major rows x cols matrices (stacked) re-laid with rows padded to an even length, the layout the
+// kernels' 16-byte pair loads require.
+template <typename T>
+std::vector<T> padded_rows(const std::vector<double> &v, int64_t rows, int64_t cols) {
+  const int64_t ld = pad_even((int)cols), n = (int64_t)v.size() / cols;
+  std::vector<T> out((size_t)(n * ld), T(0));
+  for (int64_t r = 0; r < n; ++r)
+    for (int64_t c = 0; c < cols; ++c) out[(size_t)(r * ld + c)] = (T)v[(size_t)(r * cols + c)];
+  (void)rows;
+  return out;
+}
+
 // Tile list over partitions: up to te consecutive elements of one partition per tile.
 std::vector<Tile> make_tiles(const Runner &r, const Binding &node, const Binding *face, int te, int np, int nf) {
   std::vector<Tile> t;
@@ -161,7 +173,7 @@ struct DiffOp : Op {
       require(m->rows == np && m->cols == np, R.kname + ": " + m->name + " must be Np x Np");
       d.insert(d.end(), m->mat.begin(), m->mat.end());
     }
-    auto dt = cast<T>(d);
+    auto dt = padded_rows<T>(d, 3 * np, np);
     dmat.upload(dt.data(), dt.size() * sizeof(T));
     auto tl = make_tiles(r, *u, nullptr, tile_elems(N), (int)np, 0);
     ntiles = (int)tl.size();
@@ -223,9 +235,9 @@ struct RhsOp : Op {
       require(m->rows == np && m->cols == np, R.kname + ": " + m->name + " must be Np x Np");
       d.insert(d.end(), m->mat.begin(), m->mat.end());
     }
-    auto dt = cast<T>(d);
+    auto dt = padded_rows<T>(d, 3 * np, np);
     dmat.upload(dt.data(), dt.size() * sizeof(T));
-    auto lt = cast<T>(L->mat);
+    auto lt = padded_rows<T>(L->mat, np, nf);
     lift.upload(lt.data(), lt.size() * sizeof(T));
     std::vector<int32_t> fmi(fm->mat.begin(), fm->mat.end());
     for (int32_t v : fmi) require(v >= 0 && v < np, R.kname + ": Fmask entry out of range");

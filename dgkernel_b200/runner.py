@@ -346,24 +346,26 @@ class Runner:
         self._copy(name, False, host)
 
     def CopyArrayToHost(self, name: str) -> np.ndarray:
-        """All partitions of an array, concatenated, in its device type (runner/runner_copy.go:13-80)."""
-        b = self.Bindings[name]
-        off = self.GetOffsets(name)
-        parts = [self.CopyPartitionToHost(name, p) for p in range(self.NumPartitions)]
-        del off
-        return np.concatenate(parts) if parts else np.zeros(0, _DT2NP[b.dev_dtype])
+        """All partitions of an array back to back, raw device order and type (runner/runner_copy.go:13-80).
+        Each partition contributes K[part] x values-per-element values; the reference copies only K[part]
+        values (runner/runner_copy.go:64-66)."""
+        return np.concatenate([self.CopyPartitionToHost(name, p) for p in range(self.NumPartitions)])
 
     def CopyPartitionToHost(self, name: str, part: int) -> np.ndarray:
-        """One partition (runner/runner_copy.go:83-145).  Copies K[part] x values-per-element values; the
-        reference copies only K[part] values (runner/runner_copy.go:64-66)."""
-        b = self.Bindings[name]
+        """One partition in raw device order and type (runner/runner_copy.go:83-145)."""
+        b = self.Bindings.get(name)
+        if b is None or b.is_scalar:
+            raise DGKError(3, f"array {name} not found")
         if part < 0 or part >= self.NumPartitions:
             raise DGKError(1, f"invalid partition ID: {part}")
         off = self.GetOffsets(name)
-        vpe = (off[-1] - off[0]) // max(1, sum(self.K)) if not b.partitioned else None
-        n = np.asarray(b.host[part]).size if b.partitioned else self.K[part] * vpe
-        out = np.zeros(n, dtype=_DT2NP[b.host_dtype])
-        self._check(lib().dgk_copy_partition_from_device(self._h, name.encode(), part, _ptr(out), out.nbytes))
+        total = sum(self.K)
+        if b.partitioned:
+            n = int(np.asarray(b.host[part]).size)
+        else:
+            n = (b.spec.Size // total) * self.K[part] if total else 0
+        out = np.zeros(n, dtype=_DT2NP[b.dev_dtype])
+        self._check(lib().dgk_copy_raw_from_device(self._h, name.encode(), off[part], _ptr(out), out.nbytes))
         return out
 
     # -- kernels ----------------------------------------------------------------------------------

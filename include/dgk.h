@@ -104,6 +104,9 @@ int dgk_copy_from_device(dgk_runner *r, const char *name, void *host, int64_t by
 /* One partition of a [][]T / []mat.Matrix binding (kernel_copy.go:288-560), the cgo-safe form. */
 int dgk_copy_partition_to_device(dgk_runner *r, const char *name, int32_t part, const void *host, int64_t bytes);
 int dgk_copy_partition_from_device(dgk_runner *r, const char *name, int32_t part, void *host, int64_t bytes);
+/* Raw device bytes of an array starting at a value offset, in the device type and layout (gocca
+ * Memory.CopyToWithOffset as used by CopyArrayToHost / CopyPartitionToHost, runner/runner_copy.go:13-145). */
+int dgk_copy_raw_from_device(dgk_runner *r, const char *name, int64_t value_offset, void *host, int64_t bytes);
 /* Host-side copy of `<name>_offsets` (runner/runner.go:227-254), npart+1 values. */
 int dgk_get_offsets(dgk_runner *r, const char *name, int64_t *out);
 /* Device address of `<name>_global` (or of a matrix), for zero-copy interop. */
