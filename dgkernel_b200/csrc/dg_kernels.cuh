@@ -28,7 +28,7 @@ struct Tile {
 enum : int { kStatusOk = 0, kStatusBadGather = 1 };
 
 // Even row stride of matrices as the kernels read them (pairs of entries load as one vector).
-constexpr int pad_even(int c) { return (c + 1) & ~1; }
+__host__ __device__ constexpr int pad_even(int c) { return (c + 1) & ~1; }
 
 template <int N>
 struct Order {

@@ -122,7 +122,7 @@ __device__ __forceinline__ void rows_matvec(const T *__restrict__ M, const T *xe
 #pragma unroll
     for (int r = 0; r < RG; ++r) acc[m][r] = T(0);
   const int i0 = g * RG;
-#pragma unroll 2
+#pragma unroll 1
   for (int j = 0; j + 1 < NC; j += 2) {
     T x0 = xe[j], x1 = xe[j + 1];
     if (SQUARE) {
@@ -179,7 +179,7 @@ struct Smem {
 };
 
 template <typename T, int N, bool MSMEM>
-__global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A, int rhs_only) {
+__global__ void __launch_bounds__(Cfg<N>::THREADS, 2) rhs_stage_kernel(RhsArgs<T> A, int rhs_only) {
   using O = Order<N>;
   using C = Cfg<N>;
   using S = Smem<T, N, MSMEM>;
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
   T *sd = su + S::U;
   T *sf = sd + S::D3;
   int *sfm = reinterpret_cast<int *>(sf + S::F);
-  const int tid = threadIdx.x, nth = blockDim.x;
+  const int tid = threadIdx.x, nth = C::THREADS;  // launched with exactly Cfg<N>::THREADS threads
   if (tid == 0 && blockIdx.x < A.ntiles) prefetch_tile(A, A.tiles[blockIdx.x], NP, NF);
   if (MSMEM) {  // the operator stores both matrices with the padded row strides used here
     for (int i = tid; i < S::DM; i += nth) sD[i] = A.Dmat[i];
@@ -204,62 +204,137 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
   const T a = A.a, b = A.b, dt = A.dt;
   __syncthreads();
 
+  // Per-thread item counts of the element-contiguous (flat) phases.  Each flat phase issues the loads of a
+  // whole batch before consuming any, so a tile costs a few memory round trips per phase instead of one per
+  // item; batch sizes keep the loaded values within a modest register budget.
+  constexpr int THREADS = C::THREADS;
+  constexpr int NI = (TE * NP + THREADS - 1) / THREADS;  // node items per thread
+  constexpr int NJ = (TE * NF + THREADS - 1) / THREADS;  // face items per thread
+  constexpr int WORDS = sizeof(T) / 4;                    // 32-bit registers per value
+  constexpr int CHN = (54 / (9 * WORDS)) > 0 ? (54 / (9 * WORDS)) : 1;  // metric batch (9 values per item)
+  constexpr int CHF = (40 / (4 * WORDS)) > 0 ? (40 / (4 * WORDS)) : 1;  // face-data batch (4 values per item)
+
   for (int t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
     const Tile tl = A.tiles[t];
     if (tid == 0 && t + (int)gridDim.x < A.ntiles) prefetch_tile(A, A.tiles[t + gridDim.x], NP, NF);
-    const int ne = tl.nelem;
+    const int ne = tl.nelem, nn = ne * NP, nfc = ne * NF;
     const T *ug = A.u_in + tl.node_base;
     // P0: the tile's state, coalesced
-    for (int idx = tid; idx < ne * NP; idx += nth) {
-      const int e = idx / NP, i = idx - e * NP;
-      su[e * NPS + i] = ug[idx];
+    {
+      T v[NI];
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const int idx = tid + k * THREADS;
+        v[k] = idx < nn ? ug[idx] : T(0);
+      }
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const int idx = tid + k * THREADS;
+        if (idx < nn) {
+          const int e = idx / NP, i = idx - e * NP;
+          su[e * NPS + i] = v[k];
+        }
+      }
     }
-    __syncthreads();
-    // P1: ur, us, ut (of u, or of u^2/2 in conservative form) for this thread's element and rows
-    if (e_own < ne) {
-      T acc[3][RG];
-      if (A.conservative)
-        rows_matvec<T, NP, NP, RG, 3, true>(Dm, su + e_own * NPS, g_own, acc);
-      else
-        rows_matvec<T, NP, NP, RG, 3, false>(Dm, su + e_own * NPS, g_own, acc);
+    // P0b: neighbour traces uP through the fused exchange map into the flux buffer (index batch, then gather batch)
+    {
+      int32_t src[NJ];
 #pragma unroll
-      for (int r = 0; r < RG; ++r) {
-        const int i = g_own * RG + r;
-        if (i < NP) {
+      for (int k = 0; k < NJ; ++k) {
+        const int idx = tid + k * THREADS;
+        src[k] = idx < nfc ? lds(A.gmap + tl.face_base + idx) : 0;
+      }
+      T up[NJ];
 #pragma unroll
-          for (int m = 0; m < 3; ++m) sd[m * TE * NPS + e_own * NPS + i] = acc[m][r];
+      for (int k = 0; k < NJ; ++k) {
+        const int idx = tid + k * THREADS;
+        const bool ok = src[k] >= 0 && (int64_t)src[k] < A.n_u_values;
+        up[k] = (idx < nfc && ok) ? A.u_in[src[k]] : T(0);
+        if (idx < nfc && !ok) atomicExch(A.status, kStatusBadGather);
+      }
+#pragma unroll
+      for (int k = 0; k < NJ; ++k) {
+        const int idx = tid + k * THREADS;
+        if (idx < nfc) {
+          const int e = idx / NF, q = idx - e * NF;
+          const bool ok = src[k] >= 0 && (int64_t)src[k] < A.n_u_values;
+          // a rejected index (reported above) falls back to the interior trace uM
+          sf[e * NFS + q] = ok ? up[k] : A.u_in[tl.node_base + e * NP + sfm[q]];
         }
       }
     }
     __syncthreads();
-    // P2a: volume term with the per-node metrics (coalesced streams)
-    for (int idx = tid; idx < ne * NP; idx += nth) {
-      const int e = idx / NP, i = idx - e * NP;
-      const int64_t gi = tl.node_base + idx;
-      const int so = e * NPS + i;
-      const T ur = sd[so], us = sd[TE * NPS + so], ut = sd[2 * TE * NPS + so];
-      const T ux = lds(A.geo[0] + gi) * ur + lds(A.geo[3] + gi) * us + lds(A.geo[6] + gi) * ut;
-      const T uy = lds(A.geo[1] + gi) * ur + lds(A.geo[4] + gi) * us + lds(A.geo[7] + gi) * ut;
-      const T uz = lds(A.geo[2] + gi) * ur + lds(A.geo[5] + gi) * us + lds(A.geo[8] + gi) * ut;
-      sd[so] = A.conservative ? -(ux + uy + uz) : -su[so] * (ux + uy + uz);
+    // P1: ur, us, ut (of u, or of u^2/2 in conservative form) for this thread's element and rows
+    if (e_own < ne) {
+      // one derivative matrix at a time keeps a single accumulator set live
+#pragma unroll 1
+      for (int m = 0; m < 3; ++m) {
+        T acc[1][RG];
+        if (A.conservative)
+          rows_matvec<T, NP, NP, RG, 1, true>(Dm + m * NP * Pad<NP>::V, su + e_own * NPS, g_own, acc);
+        else
+          rows_matvec<T, NP, NP, RG, 1, false>(Dm + m * NP * Pad<NP>::V, su + e_own * NPS, g_own, acc);
+#pragma unroll
+        for (int r = 0; r < RG; ++r) {
+          const int i = g_own * RG + r;
+          if (i < NP) sd[m * TE * NPS + e_own * NPS + i] = acc[0][r];
+        }
+      }
     }
-    // P2b: Lax-Friedrichs surface term at every face point; uP through the fused exchange map
-    for (int idx = tid; idx < ne * NF; idx += nth) {
-      const int e = idx / NF, q = idx - e * NF;
-      const int64_t fi = tl.face_base + idx;
-      const T uM = su[e * NPS + sfm[q]];
-      const int32_t src = lds(A.gmap + fi);
-      T uP = uM;
-      if (src >= 0 && (int64_t)src < A.n_u_values)
-        uP = A.u_in[src];
-      else
-        atomicExch(A.status, kStatusBadGather);
-      const T nsum = lds(A.face[0] + fi) + lds(A.face[1] + fi) + lds(A.face[2] + fi);
-      const T fM = T(0.5) * uM * uM * nsum, fP = T(0.5) * uP * uP * nsum;
-      const T an = fabs(nsum);
-      const T lam = fmax(fabs(uM) * an, fabs(uP) * an);
-      const T du = fM - (T(0.5) * (fM + fP) + T(0.5) * lam * (uM - uP));
-      sf[e * NFS + q] = lds(A.face[3] + fi) * du;
+    __syncthreads();
+    // P2a: volume term with the per-node metrics (coalesced streams, CHN items per batch)
+#pragma unroll
+    for (int k0 = 0; k0 < NI; k0 += CHN) {
+      T gm[CHN][9];
+#pragma unroll
+      for (int k = 0; k < CHN; ++k) {
+        const int idx = tid + (k0 + k) * THREADS;
+        if (k0 + k < NI && idx < nn) {
+#pragma unroll
+          for (int m = 0; m < 9; ++m) gm[k][m] = lds(A.geo[m] + tl.node_base + idx);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < CHN; ++k) {
+        const int idx = tid + (k0 + k) * THREADS;
+        if (k0 + k < NI && idx < nn) {
+          const int e = idx / NP, i = idx - e * NP;
+          const int so = e * NPS + i;
+          const T ur = sd[so], us = sd[TE * NPS + so], ut = sd[2 * TE * NPS + so];
+          const T ux = gm[k][0] * ur + gm[k][3] * us + gm[k][6] * ut;
+          const T uy = gm[k][1] * ur + gm[k][4] * us + gm[k][7] * ut;
+          const T uz = gm[k][2] * ur + gm[k][5] * us + gm[k][8] * ut;
+          sd[so] = A.conservative ? -(ux + uy + uz) : -su[so] * (ux + uy + uz);
+        }
+      }
+    }
+    // P2b: Lax-Friedrichs surface term at every face point (face data in CHF-item batches)
+#pragma unroll
+    for (int k0 = 0; k0 < NJ; k0 += CHF) {
+      T fc[CHF][4];
+#pragma unroll
+      for (int k = 0; k < CHF; ++k) {
+        const int idx = tid + (k0 + k) * THREADS;
+        if (k0 + k < NJ && idx < nfc) {
+#pragma unroll
+          for (int m = 0; m < 4; ++m) fc[k][m] = lds(A.face[m] + tl.face_base + idx);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < CHF; ++k) {
+        const int idx = tid + (k0 + k) * THREADS;
+        if (k0 + k < NJ && idx < nfc) {
+          const int e = idx / NF, q = idx - e * NF;
+          const T uM = su[e * NPS + sfm[q]];
+          const T uP = sf[e * NFS + q];
+          const T nsum = fc[k][0] + fc[k][1] + fc[k][2];
+          const T fM = T(0.5) * uM * uM * nsum, fP = T(0.5) * uP * uP * nsum;
+          const T an = fabs(nsum);
+          const T lam = fmax(fabs(uM) * an, fabs(uP) * an);
+          const T du = fM - (T(0.5) * (fM + fP) + T(0.5) * lam * (uM - uP));
+          sf[e * NFS + q] = fc[k][3] * du;
+        }
+      }
     }
     __syncthreads();
     // P3: rhs = volume + LIFT * (Fscale du)
@@ -274,16 +349,28 @@ __global__ void __launch_bounds__(Cfg<N>::THREADS) rhs_stage_kernel(RhsArgs<T> A
     }
     __syncthreads();
     // P4: LSERK4 stage (or the bare RHS), coalesced
-    for (int idx = tid; idx < ne * NP; idx += nth) {
-      const int e = idx / NP, i = idx - e * NP;
-      const int64_t gi = tl.node_base + idx;
-      const T rhs = sd[e * NPS + i];
-      if (rhs_only) {
-        sts(A.rhs_out + gi, rhs);
-      } else {
-        const T res = a * lds(A.resu + gi) + dt * rhs;
-        sts(A.resu + gi, res);
-        sts(A.u_out + gi, su[e * NPS + i] + b * res);
+    {
+      T rs[NI];
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const int idx = tid + k * THREADS;
+        rs[k] = (!rhs_only && idx < nn) ? lds(A.resu + tl.node_base + idx) : T(0);
+      }
+#pragma unroll
+      for (int k = 0; k < NI; ++k) {
+        const int idx = tid + k * THREADS;
+        if (idx < nn) {
+          const int e = idx / NP, i = idx - e * NP;
+          const int64_t gi = tl.node_base + idx;
+          const T rhs = sd[e * NPS + i];
+          if (rhs_only) {
+            sts(A.rhs_out + gi, rhs);
+          } else {
+            const T res = a * rs[k] + dt * rhs;
+            sts(A.resu + gi, res);
+            sts(A.u_out + gi, su[e * NPS + i] + b * res);
+          }
+        }
       }
     }
     __syncthreads();

@@ -18,6 +18,14 @@ template <typename T>
 void launch_update(const Tile *tiles, int ntiles, int np, T *u, T *resu, const T *rhs, double c0, double c1, double c2,
                    int mode, int num_sms, cudaStream_t st);
 int tile_elems(int N);
+// TMA-pipelined form of the fused stage (kernels_tma.cu); returns false when the order has no TMA form.
+template <typename T>
+bool launch_rhs_tma(int N, const RhsArgs<T> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info);
+template <typename T>
+int tma_tile_elems(int N);  // 0 when the order has no TMA form
+// FP64 form with TMA streaming and the element-local products on the FP64 tensor path (kernels_tma.cu).
+bool launch_rhs_dmma(int N, const RhsArgs<double> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info);
+int dmma_tile_elems(int N);  // 0 when the order has no such form
 
 // Generic MATMUL_<M> over partitions: out[e*rows + i] (+)= sum_j M[i][j] in[e*cols + j].
 template <typename T>

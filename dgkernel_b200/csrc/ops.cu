@@ -3,8 +3,10 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
+#include <type_traits>
 
 #include "kernels.hpp"
 #include "runner.hpp"
@@ -242,10 +244,32 @@ struct RhsOp : Op {
     std::vector<int32_t> fmi(fm->mat.begin(), fm->mat.end());
     for (int32_t v : fmi) require(v >= 0 && v < np, R.kname + ": Fmask entry out of range");
     fmask.upload(fmi.data(), fmi.size() * sizeof(int32_t));
-    auto tl = make_tiles(r, *u, face[0], tile_elems(N), (int)np, nf);
-    ntiles = (int)tl.size();
-    tiles.upload(tl.data(), tl.size() * sizeof(Tile));
+    // TMA-pipelined form when the order has one and every tile's streams start on 16-byte boundaries
+    // (cp.async.bulk requirement); otherwise the register-staged form.
+    // FP64: TMA streaming + element-local products on the FP64 tensor path; FP32: register-staged form.
+    const char *no_tma = std::getenv("DGK_DISABLE_TMA");
+    const bool tma_ok = !(no_tma && no_tma[0] == '1') && std::is_same<T, double>::value;
+    const int te_tma = tma_ok ? dmma_tile_elems(N) : 0;
+    use_tma = false;
+    if (te_tma > 0) {
+      auto tl = make_tiles(r, *u, face[0], te_tma, (int)np, nf);
+      bool aligned = true;
+      for (const Tile &x : tl)
+        aligned = aligned && (x.node_base * (int64_t)sizeof(T)) % 16 == 0 &&
+                  (x.face_base * (int64_t)sizeof(T)) % 16 == 0 && (x.face_base * 4) % 16 == 0;
+      if (aligned) {
+        use_tma = true;
+        ntiles = (int)tl.size();
+        tiles.upload(tl.data(), tl.size() * sizeof(Tile));
+      }
+    }
+    if (!use_tma) {
+      auto tl = make_tiles(r, *u, face[0], tile_elems(N), (int)np, nf);
+      ntiles = (int)tl.size();
+      tiles.upload(tl.data(), tl.size() * sizeof(Tile));
+    }
   }
+  bool use_tma = false;
   std::vector<std::string> scalar_names() const override {
     if (rhs_only) return {};
     return {"a", "b", "dt"};
@@ -272,7 +296,10 @@ struct RhsOp : Op {
     }
     A.conservative = conservative;
     A.status = r.status_word();
-    launch_rhs<T>(N, A, rhs_only, r.num_sms, r.stream(), &info);
+    bool done = false;
+    if constexpr (std::is_same<T, double>::value)
+      if (use_tma) done = launch_rhs_dmma(N, A, rhs_only, r.num_sms, r.stream(), &info);
+    if (!done) launch_rhs<T>(N, A, rhs_only, r.num_sms, r.stream(), &info);
     if (!rhs_only) std::swap(u->dptr, unext->dptr);  // "u" always names the newest state
   }
 };
