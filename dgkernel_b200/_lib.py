@@ -51,6 +51,7 @@ SIGNATURES = {
     "dgk_setup_geometry": [_P, _P, _I64, _PD, _PD, _PD, _PI64, _PI64, _PI64, _D, C.POINTER(_S), _PD],
     "dgk_init_field": [_P, _S, _S, _S, _S, _I32, _D, _D, _I32, _PD],
     "dgk_splitmix_uniform": [_U64, _I64, _PD],
+    "dgk_convert_upload_noalloc": [_P, _I32, _P, _I32, _I64, _P],
 }
 _STRING_RESULT = {"dgk_last_error", "dgk_global_error"}
 

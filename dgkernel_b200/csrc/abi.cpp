@@ -46,6 +46,8 @@ int copy_text(const std::string &s, char *buf, int64_t len) {
 }
 }  // namespace
 
+void dgk::set_global_error(const std::string &msg) { g_error = msg; }
+
 extern "C" {
 
 int dgk_runner_create(const int64_t *K, int32_t npart, int32_t int_type, dgk_runner **out) {

@@ -23,6 +23,8 @@ struct Error : std::runtime_error {
 };
 
 void cuda_check(cudaError_t e, const char *what);
+// Message returned by dgk_global_error() for calls made without a runner.
+void set_global_error(const std::string &msg);
 
 // Values of the device status word (kernels write them, the host reads them; nothing traps).
 constexpr int kStatusGatherCode = 1;   // a face gather index was out of range

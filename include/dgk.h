@@ -185,6 +185,19 @@ int dgk_init_field(dgk_runner *r, const char *name, const char *xname, const cha
 /* splitmix64 uniform stream (53-bit doubles), for reproducible inputs across host and oracle. */
 int dgk_splitmix_uniform(uint64_t seed, int64_t count, double *out);
 
+/* ---- allocation-free upload ----------------------------------------------------------------------- */
+/* No counterpart in the reference.  Converting upload that allocates nothing: `count` host values of
+ * host_dtype are staged in a fixed 8 MiB array inside the library's device image and converted on the GPU
+ * into `device_dst` (dev_dtype), on `cuda_stream` (NULL = legacy default stream); the call returns after the
+ * stream has finished.  For callers that must not allocate device memory once running -- a host application
+ * that owns the device-memory budget, or a time-stepping loop that cannot absorb a cudaMalloc's latency and
+ * implicit synchronisation -- unlike dgk_copy_to_device, whose staging buffer grows with cudaMalloc.  More than 8 MiB of host data is rejected
+ * with DGK_ERR_INVALID (split the upload).  The first call on each device resolves the array's device
+ * address, so make it before any stream capture.  All calls share the array: calls that overlap on the GPU
+ * race.  Errors are reported through dgk_global_error(). */
+int dgk_convert_upload_noalloc(const void *host, int32_t host_dtype, void *device_dst, int32_t dev_dtype,
+                               int64_t count, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
