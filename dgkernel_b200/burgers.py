@@ -13,7 +13,7 @@ import numpy as np
 
 from . import mesh as M
 from .element import Element
-from .runner import (Config, Float32, Float64, INT32, INT64, Runner, Scalar, Temp, Input)
+from .runner import (Config, Float32, Float64, INT32, INT64, Runner, Scalar, Temp, Input, WarpAlign)
 from ._lib import check, lib
 
 import ctypes as C
@@ -66,13 +66,28 @@ def random_modes(seed: int, nmodes: int = 8, kmax: int = 3, sigma: float = 0.1) 
     return np.array(rows, dtype=np.float64)
 
 
+def bary_matrix(el) -> np.ndarray:
+    """Np x 4 barycentric coordinates (vertices A=(-1,-1,-1), B=(1,-1,-1), C=(-1,1,-1), D=(-1,-1,1)) of the
+    element's nodes; the mixed stage subtracts the linear interpolant through the vertex nodes with them."""
+    r, s, t = el.r, el.s, el.t
+    return np.stack((-(1 + r + s + t) / 2, (1 + r) / 2, (1 + s) / 2, (1 + t) / 2), axis=1)
+
+
+MIXED = "mixed"
+
+
 class BurgersProblem:
-    """Device-resident Burgers problem of order N on an n^3 x 6 Kuhn mesh with nslab x-slab partitions."""
+    """Device-resident Burgers problem of order N on an n^3 x 6 Kuhn mesh with nslab x-slab partitions.
+
+    dtype float64 / float32: the plain stage (`rhsStage`) with state, metrics and face data in that type.
+    dtype "mixed": the mixed-precision stage (`rhsStageMixed`): compensated FP32 state uhi + ulo, FP32
+    residual, compact affine geometry derived from the FP64 metrics; `get("u")` joins the pair in FP64."""
 
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
                  cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None):
         self.N, self.n, self.nslab = N, n, nslab
-        self.dtype = np.dtype(dtype)
+        self.mixed = isinstance(dtype, str) and dtype == MIXED
+        self.dtype = np.dtype(np.float64) if self.mixed else np.dtype(dtype)
         dt_code = Float64 if self.dtype == np.float64 else Float32
         el = self.el = Element(N)
         Np, Nfp = el.Np, el.Nfp
@@ -84,9 +99,15 @@ class BurgersProblem:
         self.Kpart = [K // nslab] * nslab
         r = self.runner = Runner(Config(K=self.Kpart), stream=stream)
         sn = el.ShortName
-        params = [Temp(nm).Type(dt_code).Size(K * Np) for nm in ("u", "uNext", "resu", "X", "Y", "Z") + GEO]
+        state = ("u", "X", "Y", "Z") if self.mixed else ("u", "uNext", "resu", "X", "Y", "Z")
+        params = [Temp(nm).Type(dt_code).Size(K * Np) for nm in state + GEO]
         params += [Temp(nm).Type(dt_code).Size(K * NF) for nm in FACE]
         params += [Temp("gmap").Type(INT32).Size(K * NF), Temp("vmapP").Type(INT64).Size(K * NF)]
+        if self.mixed:
+            # 128-byte partition starts: the mixed stage streams each partition's slots with 16-byte bulk copies
+            params += [Temp(nm).Type(Float32).Size(K * Np).Align(WarpAlign)
+                       for nm in ("uhi", "ulo", "uhiNext", "uloNext", "resu")]
+            params += [Input(f"Bary_{sn}").Bind(bary_matrix(el)).ToMatrix().Static()]
         params += [Input(f"{m}_{sn}").Bind(getattr(el, m)).ToMatrix().Static() for m in ("Dr", "Ds", "Dt", "LIFT")]
         params += [Input("Fmask").Bind(el.Fmask.astype(np.float64)).ToMatrix().DeviceMemType(INT32)]
         params += [Scalar("a").Type(Float64), Scalar("b").Type(Float64), Scalar("dt").Type(Float64)]
@@ -104,7 +125,7 @@ class BurgersProblem:
         # FaceConnector pick/place fused into one gather map over the state array's partition offsets
         self.vmapP = np.zeros(K * NF, dtype=np.int64)
         r.CopyFromDevice("vmapP", self.vmapP)
-        self.node_off = r.GetOffsets("u")
+        self.node_off = r.GetOffsets("uhi" if self.mixed else "u")
         self.gmap = M.face_gather_map(K, 4, Nfp, Np, self.vmapP, EToP, self.node_off)
         r.CopyToDevice("gmap", self.gmap)
         # initial condition
@@ -115,11 +136,22 @@ class BurgersProblem:
             kind, mean, amp = kinds[u0]
             modes = random_modes(seed) if kind == 2 else np.zeros((0, 5))
             check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, len(modes), _pd(modes)), r._h)
+        fixed_m = [f"Dr_{sn}", f"Ds_{sn}", f"Dt_{sn}", f"LIFT_{sn}", "Fmask"]
+        if self.mixed:
+            r.ConfigureKernel("splitState", r.Param("u"), r.Param("uhi"), r.Param("ulo"))
+            r.BuildKernel("splitState", "splitState")
+            r.ConfigureKernel("joinState", r.Param("u"), r.Param("uhi"), r.Param("ulo"))
+            r.BuildKernel("joinState", "joinState")
+            r.ExecuteKernel("splitState")
+            fixed = ["uhi", "ulo", "uhiNext", "uloNext", "resu", *GEO, *FACE, "gmap", *fixed_m, f"Bary_{sn}"]
+            op = f"rhsStageMixed(conservative={conservative})"
+        else:
+            fixed = ["u", "uNext", "resu", *GEO, *FACE, "gmap", *fixed_m]
+            op = f"rhsStage(conservative={conservative})"
         self.u0 = self.get("u")
         self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))
-        fixed = ["u", "uNext", "resu", *GEO, *FACE, "gmap", f"Dr_{sn}", f"Ds_{sn}", f"Dt_{sn}", f"LIFT_{sn}", "Fmask"]
         r.ConfigureKernel("rhsStage", *[r.Param(p) for p in fixed], r.Param("a"), r.Param("b"), r.Param("dt"))
-        r.BuildKernel(f"rhsStage(conservative={conservative})", "rhsStage")
+        r.BuildKernel(op, "rhsStage")
         self.stage = 0
 
     @property
@@ -127,14 +159,20 @@ class BurgersProblem:
         return self.K * self.el.Np
 
     def get(self, name: str) -> np.ndarray:
+        if self.mixed and name == "u":
+            self.runner.ExecuteKernel("joinState")
         n = self.K * (self.el.Np if name not in FACE + ("gmap", "vmapP") else 4 * self.el.Nfp)
         dt = {"gmap": np.int32, "vmapP": np.int64}.get(name, self.dtype)
+        if self.mixed and name in ("uhi", "ulo", "resu", "uhiNext", "uloNext"):
+            dt = np.float32
         out = np.zeros(n, dtype=dt)
         self.runner.CopyFromDevice(name, out)
         return out
 
     def set(self, name: str, host: np.ndarray):
         self.runner.CopyToDevice(name, np.ascontiguousarray(host))
+        if self.mixed and name == "u":
+            self.runner.ExecuteKernel("splitState")
 
     def run_stages(self, nstages: int):
         """Advance by nstages LSERK4 stages (stage index continues across calls)."""

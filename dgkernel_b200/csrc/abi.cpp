@@ -230,6 +230,22 @@ int dgk_face_gather_map(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, cons
   return guard(nullptr, [&] { dgk::face_gather_map(K, Nfaces, Nfp, Np, vmapP, EToP, npart, node_off, gmap); });
 }
 
+int dgk_compact_faces(int32_t npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,
+                      int32_t Np, int32_t Nfp, const int32_t *gmap, int32_t *conn_out, uint8_t *table_out,
+                      int32_t table_cap, int32_t *ncodes_out) {
+  return guard(nullptr, [&] {
+    if (npart < 1 || !K || !node_off || !face_off || !gmap || !conn_out || !ncodes_out)
+      throw dgk::Error(DGK_ERR_INVALID, "compact faces: null argument or npart < 1");
+    std::vector<int64_t> sp((size_t)npart + 1, 0);
+    for (int p = 0; p < npart; ++p) sp[(size_t)p + 1] = sp[(size_t)p] + dgk::slot_padded(K[p]);
+    dgk::CompactFaces cf = dgk::compact_faces(npart, K, node_off, face_off, sp.data(), Np, Nfp, gmap);
+    std::copy(cf.conn.begin(), cf.conn.end(), conn_out);
+    *ncodes_out = cf.ncodes;
+    if (cf.ncodes > table_cap) throw dgk::Error(DGK_ERR_INVALID, "compact faces: table_cap too small");
+    if (table_out) std::copy(cf.table.begin(), cf.table.end(), table_out);
+  });
+}
+
 int dgk_splitmix_uniform(uint64_t seed, int64_t count, double *out) {
   uint64_t s = seed;
   for (int64_t i = 0; i < count; ++i) out[i] = dgk::splitmix_uniform(s);

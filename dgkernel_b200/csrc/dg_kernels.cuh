@@ -90,4 +90,59 @@ struct DiffArgs {
   const T *Dmat;  // [3][NP][pad(NP)], rows padded to an even length
 };
 
+// ---- mixed-precision stage (mixed.cu) ----
+constexpr int kMixedSlotElems = 32;  // elements per ring slot (one per lane of a consumer warp)
+constexpr int kMixedGeoWords = 8;    // cr, cs, ct, g_0..g_3, pad
+constexpr int kMixedConnWords = 5;   // neighbour base per face, 4 packed 8-bit face-order codes
+
+struct MTile {
+  int64_t node_base;  // value index of the slot's first node in the hi/lo/resu arrays
+  int64_t elem_slot;  // index of the slot's first element in the compact geometry/connectivity arrays
+  int32_t nelem;      // elements in the slot (<= kMixedSlotElems)
+  int32_t part;       // partition (or instance)
+};
+
+struct MixedArgs {
+  const MTile *tiles;
+  int ntiles;
+  const float *uhi_in, *ulo_in;  // state read by this stage (hi also supplies the neighbour traces)
+  float *uhi_out, *ulo_out;      // state written by this stage (ping-pong partners)
+  float *resu;                   // LSERK residual, updated in place
+  const float *geo;              // kMixedGeoWords per element slot
+  const int32_t *conn;           // kMixedConnWords per element slot
+  int64_t n_u_values;            // bound of every gathered value index
+  const float *Dm;               // [NP][NPJ][3]: Dr, Ds, Dt entries interleaved per column, zero-padded
+  const float *lift;             // [NP][4 Nfp]
+  const double *bary;            // [NP][3] barycentric weights of vertices B, C, D at each node
+  const int32_t *vtx;            // node index of vertices A, B, C, D
+  const uint8_t *ftab;           // [ncodes][Nfp] neighbour-local node index of each face point
+  const int32_t *fmask;          // [4 Nfp]
+  int ncodes, ns;                // face-order codes in use; ring slots (set by the launcher)
+  float a, dt;                   // LSERK coefficients
+  double b;
+  int conservative;
+  int *status;
+};
+
+template <typename T>
+struct CompactGeoArgs {
+  int npart, np, nf;
+  int64_t elem_total;
+  const int64_t *elem_prefix;  // device, npart+1: first global element of each partition
+  const int64_t *slot_prefix;  // device, npart: first element slot of each partition (slot-padded)
+  const int64_t *node_off;     // device, npart: value offset of each partition in the metric arrays
+  const int64_t *face_off;     // device, npart: value offset of each partition in the face arrays
+  const T *geo[9];             // rx, ry, rz, sx, sy, sz, tx, ty, tz
+  const T *face[4];            // nx, ny, nz, Fscale
+  float *out;                  // kMixedGeoWords per slot
+  int *bad;                    // count of elements that are not affine within 1e-9
+};
+
+struct SplitJoinArgs {
+  int npart, join;  // join = 0: u -> (hi, lo);  join = 1: (hi, lo) -> u
+  const int64_t *count, *u_off, *hi_off, *lo_off;  // device, npart each (values)
+  double *u;
+  float *hi, *lo;
+};
+
 }  // namespace dgk

@@ -27,6 +27,13 @@ int tma_tile_elems(int N);  // 0 when the order has no TMA form
 bool launch_rhs_dmma(int N, const RhsArgs<double> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info);
 int dmma_tile_elems(int N);  // 0 when the order has no such form
 
+// Mixed-precision stage (mixed.cu); returns false when the order has no such form.
+bool launch_rhs_mixed(int N, const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info);
+uint32_t mixed_slot_bytes(int N);  // 0 when the order has no such form
+template <typename T>
+void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);
+void launch_split_join(const SplitJoinArgs &a, cudaStream_t st);
+
 // Generic MATMUL_<M> over partitions: out[e*rows + i] (+)= sum_j M[i][j] in[e*cols + j].
 template <typename T>
 void launch_matmul(const T *M_rowmajor, int rows, int cols, const T *in, T *out, const int64_t *d_in_off,

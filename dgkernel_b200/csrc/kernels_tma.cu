@@ -14,54 +14,11 @@
 #include <type_traits>
 
 #include "dg_kernels.cuh"
+#include "tma.cuh"
 #include "kernels.hpp"
 #include "runner.hpp"
 
 namespace dgk {
-
-namespace {
-
-__device__ __forceinline__ uint32_t saddr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(saddr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait: true when the phase with this parity completed, false after `limit` polls.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint32_t limit) {
-  for (uint32_t i = 0; i < limit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   saddr(dst)),
-               "l"(src), "r"(bytes), "r"(saddr(bar))
-               : "memory");
-}
-
-constexpr uint32_t kSpinLimit = 1u << 26;  // polls; a healthy stage completes in microseconds
-
-__host__ __device__ constexpr uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
-
-}  // namespace
 
 // Tile shape of the TMA form: TE elements per tile, RG rows per thread in the element-local products.
 template <typename T, int N>
@@ -400,9 +357,6 @@ __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
-}
 
 // Barrier among the consumer warps only (named barrier 1), and its AND-reduction form.
 template <int CONS>

@@ -3,6 +3,7 @@
 #include "mesh.hpp"
 
 #include <algorithm>
+#include <map>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -145,6 +146,50 @@ void face_gather_map(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmap
         gmap[face_base[dst] + pl[i]] = (int32_t)v;
       }
     }
+}
+
+int64_t slot_padded(int64_t k) { return (k + 31) / 32 * 32; }
+
+CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,
+                           const int64_t *slot_prefix, int Np, int Nfp, const int32_t *gmap) {
+  if (Np > 255) throw std::runtime_error("compact faces: Np above 255 does not fit the 8-bit table");
+  CompactFaces out;
+  out.conn.assign((size_t)(slot_prefix[npart] * 5), 0);
+  std::map<std::vector<uint8_t>, int> codes;
+  std::vector<uint8_t> order((size_t)Nfp);
+  const int64_t NF = 4 * (int64_t)Nfp;
+  for (int p = 0; p < npart; ++p)
+    for (int64_t e = 0; e < K[p]; ++e) {
+      uint32_t packed = 0;
+      for (int f = 0; f < 4; ++f) {
+        const int32_t *g = gmap + face_off[p] + e * NF + (int64_t)f * Nfp;
+        // partition holding the first face point, then the element base within it
+        const int q = (int)(std::upper_bound(node_off, node_off + npart, (int64_t)g[0]) - node_off) - 1;
+        if (q < 0 || g[0] >= node_off[q] + K[q] * Np) throw std::runtime_error("compact faces: gather index outside every partition of the state");
+        const int64_t base = node_off[q] + (g[0] - node_off[q]) / Np * Np;
+        if (base > INT32_MAX) throw std::runtime_error("compact faces: neighbour base exceeds int32");
+        for (int i = 0; i < Nfp; ++i) {
+          const int64_t j = (int64_t)g[i] - base;
+          if (j < 0 || j >= Np) throw std::runtime_error("compact faces: the points of one face span two elements");
+          order[(size_t)i] = (uint8_t)j;
+        }
+        auto it = codes.find(order);
+        int code;
+        if (it == codes.end()) {
+          code = (int)codes.size();
+          if (code > 254) throw std::runtime_error("compact faces: more than 255 distinct face orders");
+          codes.emplace(order, code);
+          out.table.insert(out.table.end(), order.begin(), order.end());
+        } else {
+          code = it->second;
+        }
+        out.conn[(size_t)((slot_prefix[p] + e) * 5 + f)] = (int32_t)base;
+        packed |= (uint32_t)code << (8 * f);
+      }
+      out.conn[(size_t)((slot_prefix[p] + e) * 5 + 4)] = (int32_t)packed;
+    }
+  out.ncodes = (int)codes.size();
+  return out;
 }
 
 uint64_t splitmix_next(uint64_t &state) {

@@ -19,6 +19,20 @@ FaceConnector face_connector(int64_t K, int Nfaces, int Nfp, int Np, const int64
                              int npart);
 void face_gather_map(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmapP, const int64_t *EToP, int npart,
                      const int64_t *node_off, int32_t *gmap);
+// Gather map compressed to one neighbour base per face plus a face-order code (the mixed stage's layout).
+// Elements of partition p occupy slots slot_prefix[p] .. slot_prefix[p] + K[p] - 1; each slot holds
+// conn[5*slot + f] = value index of the face-f neighbour's first node and conn[5*slot + 4] = the four 8-bit
+// codes; table[code*Nfp + i] = node index of face point i within the neighbour.  Throws when a face's points
+// do not lie in one element of the state layout, when a base exceeds int32, or past 255 distinct orders.
+struct CompactFaces {
+  std::vector<int32_t> conn;
+  std::vector<uint8_t> table;
+  int ncodes = 0;
+};
+CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,
+                           const int64_t *slot_prefix, int Np, int Nfp, const int32_t *gmap);
+int64_t slot_padded(int64_t k);  // k rounded up to whole 32-element slots
+
 uint64_t splitmix_next(uint64_t &state);
 double splitmix_uniform(uint64_t &state);
 

@@ -9,6 +9,7 @@
 #include <type_traits>
 
 #include "kernels.hpp"
+#include "mesh.hpp"
 #include "runner.hpp"
 
 namespace dgk {
@@ -362,6 +363,225 @@ struct MatmulOp : Op {
   }
 };
 
+
+// Mixed-precision stage (mixed.cu): compensated FP32 state (uhi + ulo), FP32 residual, compact affine
+// geometry and compressed face maps, both derived here once from the per-node arrays and the gather map that
+// the plain rhsStage reads.  Roles: uhi, ulo, uhiNext, uloNext, resu (float32 node arrays); Rx..Tz, nx, ny,
+// nz, Fscale (float64 or float32, read at build time only); gmap (int32, value indices into uhi's layout);
+// matrices Dr, Ds, Dt, LIFT, Fmask and Bary (Np x 4 barycentric coordinates of the nodes).
+struct MixedOp : Op {
+  int N = 0, ntiles = 0, conservative = 0, ncodes = 0;
+  Binding *uhi, *ulo, *uhin, *ulon, *resu;
+  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask;
+  LaunchInfo info;
+
+  template <typename G>
+  void compact_geometry(Runner &r, Binding *const *geo, Binding *const *face, const std::vector<int64_t> &slot_prefix,
+                        int np, int nf, const std::string &kname) {
+    const int P = r.npart;
+    std::vector<int64_t> ep(P + 1, 0);
+    for (int p = 0; p < P; ++p) ep[p + 1] = ep[p] + r.K[p];
+    DevBuf dep, dsp, dno, dfo, dbad;
+    dep.upload(ep.data(), sizeof(int64_t) * (P + 1));
+    dsp.upload(slot_prefix.data(), sizeof(int64_t) * P);
+    dno.upload(geo[0]->offsets.data(), sizeof(int64_t) * P);
+    dfo.upload(face[0]->offsets.data(), sizeof(int64_t) * P);
+    int zero = 0;
+    dbad.upload(&zero, sizeof(int));
+    CompactGeoArgs<G> g{};
+    g.npart = P;
+    g.np = np;
+    g.nf = nf;
+    g.elem_total = ep[P];
+    g.elem_prefix = dep.get<int64_t>();
+    g.slot_prefix = dsp.get<int64_t>();
+    g.node_off = dno.get<int64_t>();
+    g.face_off = dfo.get<int64_t>();
+    for (int i = 0; i < 9; ++i) g.geo[i] = reinterpret_cast<const G *>(geo[i]->dptr);
+    for (int i = 0; i < 4; ++i) g.face[i] = reinterpret_cast<const G *>(face[i]->dptr);
+    g.out = geoE.get<float>();
+    g.bad = dbad.get<int>();
+    launch_compact_geometry<G>(g, r.stream());
+    int bad = 0;
+    cuda_check(cudaMemcpyAsync(&bad, dbad.p, sizeof(int), cudaMemcpyDeviceToHost, r.stream()), "read affinity check");
+    cuda_check(cudaStreamSynchronize(r.stream()), "compact geometry");
+    if (bad)
+      throw Error(DGK_ERR_UNSUPPORTED, kname + ": the mixed stage needs straight-sided elements; " + std::to_string(bad) +
+                                           " elements have non-constant metrics or face factors");
+  }
+
+  MixedOp(Runner &r, Roles &R) {
+    static const char *gn[9] = {"Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz"};
+    static const char *fn[4] = {"nx", "ny", "nz", "Fscale"};
+    conservative = R.flag("conservative", 0);
+    uhi = R.array("uhi");
+    ulo = R.array("ulo");
+    uhin = R.array("uhiNext");
+    ulon = R.array("uloNext");
+    resu = R.array("resu");
+    require(uhi->dev_dtype == DGK_FLOAT32, R.kname + ": uhi must be float32 on the device");
+    for (Binding *b : {ulo, uhin, ulon, resu}) same_layout(*uhi, *b, R.kname);
+    Binding *geo[9], *face[4];
+    for (int i = 0; i < 9; ++i) geo[i] = R.array(gn[i]);
+    for (int i = 0; i < 4; ++i) face[i] = R.array(fn[i]);
+    Binding *gmap = R.array("gmap");
+    Binding *Dr = R.matrix("Dr"), *Ds = R.matrix("Ds"), *Dt = R.matrix("Dt"), *L = R.matrix("LIFT"),
+            *fm = R.matrix("Fmask"), *B = R.matrix("Bary");
+    const int64_t np = Dr->rows;
+    N = order_from_np(np);
+    if (mixed_slot_bytes(N) == 0)
+      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the mixed stage is built for orders 1..5");
+    const int nfp = (N + 1) * (N + 2) / 2, nf = 4 * nfp;
+    require(uhi->values_per_elem == np, R.kname + ": uhi must hold Np values per element");
+    for (Binding *m : {Dr, Ds, Dt}) require(m->rows == np && m->cols == np, R.kname + ": " + m->name + " must be Np x Np");
+    require(L->rows == np && L->cols == nf, R.kname + ": LIFT must be Np x 4Nfp");
+    require(fm->rows * fm->cols == nf, R.kname + ": Fmask must hold 4*Nfp entries");
+    require(B->rows == np && B->cols == 4, R.kname + ": Bary must be Np x 4");
+    require(geo[0]->values_per_elem == np, R.kname + ": metric arrays must hold Np values per element");
+    for (Binding *b : geo) same_layout(*geo[0], *b, R.kname);
+    require(face[0]->values_per_elem == nf, R.kname + ": face arrays must hold 4*Nfp values per element");
+    for (Binding *b : face) same_layout(*face[0], *b, R.kname);
+    require(geo[0]->dev_dtype == face[0]->dev_dtype &&
+                (geo[0]->dev_dtype == DGK_FLOAT64 || geo[0]->dev_dtype == DGK_FLOAT32),
+            R.kname + ": metric and face arrays must share a float device type");
+    require(gmap->dev_dtype == DGK_INT32 && gmap->values_per_elem == nf,
+            R.kname + ": gmap must be int32 with 4*Nfp values per element");
+    const int P = r.npart;
+    std::vector<int64_t> slot_prefix(P + 1, 0);
+    for (int p = 0; p < P; ++p) slot_prefix[p + 1] = slot_prefix[p] + slot_padded(r.K[p]);
+    const int64_t nslots = std::max<int64_t>(slot_prefix[P], 1);
+    {
+      std::vector<float> z((size_t)(nslots * kMixedGeoWords), 0.f);
+      geoE.upload(z.data(), z.size() * sizeof(float));
+    }
+    if (geo[0]->dev_dtype == DGK_FLOAT64)
+      compact_geometry<double>(r, geo, face, slot_prefix, (int)np, nf, R.kname);
+    else
+      compact_geometry<float>(r, geo, face, slot_prefix, (int)np, nf, R.kname);
+    // gather map -> neighbour base + face-order code per face (exact: the table reproduces every entry)
+    std::vector<int32_t> gm((size_t)gmap->offsets.back());
+    cuda_check(cudaMemcpy(gm.data(), gmap->dptr, gm.size() * sizeof(int32_t), cudaMemcpyDeviceToHost), "read gmap");
+    CompactFaces cf;
+    try {
+      cf = compact_faces(P, r.K.data(), uhi->offsets.data(), gmap->offsets.data(), slot_prefix.data(), (int)np, nfp,
+                         gm.data());
+    } catch (const std::exception &ex) {
+      throw Error(DGK_ERR_INVALID, R.kname + ": " + ex.what());
+    }
+    ncodes = std::max(cf.ncodes, 1);
+    if (cf.table.empty()) cf.table.assign((size_t)nfp, 0);
+    conn.upload(cf.conn.data(), std::max<size_t>(cf.conn.size(), 1) * sizeof(int32_t));
+    ftab.upload(cf.table.data(), cf.table.size());
+    // Dr, Ds, Dt interleaved per column ([i][j][r,s,t]), columns padded to a multiple of 4 with zeros
+    const int npj = ((int)np + 3) & ~3;
+    std::vector<float> d((size_t)(np * npj * 3), 0.f);
+    for (int64_t i = 0; i < np; ++i)
+      for (int64_t j = 0; j < np; ++j) {
+        d[(size_t)((i * npj + j) * 3 + 0)] = (float)Dr->mat[(size_t)(i * np + j)];
+        d[(size_t)((i * npj + j) * 3 + 1)] = (float)Ds->mat[(size_t)(i * np + j)];
+        d[(size_t)((i * npj + j) * 3 + 2)] = (float)Dt->mat[(size_t)(i * np + j)];
+      }
+    dm.upload(d.data(), d.size() * sizeof(float));
+    auto lt = cast<float>(L->mat);
+    lift.upload(lt.data(), lt.size() * sizeof(float));
+    std::vector<double> bw((size_t)(np * 3));
+    int32_t vt[4];
+    for (int c = 0; c < 4; ++c) {
+      int64_t best = 0;
+      for (int64_t i = 0; i < np; ++i)
+        if (B->mat[(size_t)(i * 4 + c)] > B->mat[(size_t)(best * 4 + c)]) best = i;
+      require(std::fabs(B->mat[(size_t)(best * 4 + c)] - 1.0) < 1e-10, R.kname + ": Bary has no vertex node");
+      vt[c] = (int32_t)best;
+    }
+    for (int64_t i = 0; i < np; ++i)
+      for (int c = 0; c < 3; ++c) bw[(size_t)(i * 3 + c)] = B->mat[(size_t)(i * 4 + c + 1)];
+    bary.upload(bw.data(), bw.size() * sizeof(double));
+    vtx.upload(vt, sizeof(vt));
+    std::vector<int32_t> fmi(fm->mat.begin(), fm->mat.end());
+    for (int32_t v : fmi) require(v >= 0 && v < np, R.kname + ": Fmask entry out of range");
+    fmask.upload(fmi.data(), fmi.size() * sizeof(int32_t));
+    std::vector<MTile> tl;
+    for (int p = 0; p < P; ++p)
+      for (int64_t s0 = 0; s0 < r.K[p]; s0 += kMixedSlotElems) {
+        MTile x;
+        x.node_base = uhi->offsets[p] + s0 * np;
+        x.elem_slot = slot_prefix[p] + s0;
+        x.nelem = (int32_t)std::min<int64_t>(kMixedSlotElems, r.K[p] - s0);
+        x.part = p;
+        require((x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
+        tl.push_back(x);
+      }
+    ntiles = (int)tl.size();
+    tiles.upload(tl.data(), std::max<size_t>(tl.size(), 1) * sizeof(MTile));
+  }
+  std::vector<std::string> scalar_names() const override { return {"a", "b", "dt"}; }
+  void launch(Runner &r, const std::vector<double> &s) override {
+    if (ntiles == 0) return;
+    MixedArgs A{};
+    A.tiles = tiles.get<MTile>();
+    A.ntiles = ntiles;
+    A.uhi_in = reinterpret_cast<const float *>(uhi->dptr);
+    A.ulo_in = reinterpret_cast<const float *>(ulo->dptr);
+    A.uhi_out = reinterpret_cast<float *>(uhin->dptr);
+    A.ulo_out = reinterpret_cast<float *>(ulon->dptr);
+    A.resu = reinterpret_cast<float *>(resu->dptr);
+    A.geo = geoE.get<float>();
+    A.conn = conn.get<int32_t>();
+    A.n_u_values = uhi->offsets.back();
+    A.Dm = dm.get<float>();
+    A.lift = lift.get<float>();
+    A.bary = bary.get<double>();
+    A.vtx = vtx.get<int32_t>();
+    A.ftab = ftab.get<uint8_t>();
+    A.fmask = fmask.get<int32_t>();
+    A.ncodes = ncodes;
+    A.a = (float)s[0];
+    A.b = s[1];
+    A.dt = (float)s[2];
+    A.conservative = conservative;
+    A.status = r.status_word();
+    if (!launch_rhs_mixed(N, A, r.num_sms, r.stream(), &info))
+      throw Error(DGK_ERR_UNSUPPORTED, "mixed stage: no launch shape fits shared memory for this order");
+    std::swap(uhi->dptr, uhin->dptr);  // "uhi"/"ulo" always name the newest state
+    std::swap(ulo->dptr, ulon->dptr);
+  }
+};
+
+// State split u (float64) -> uhi + ulo (float32 pair) and the join back, per partition.
+struct SplitJoinOp : Op {
+  int join;
+  Binding *u, *hi, *lo;
+  DevBuf cnt, uo, ho, lo_off;
+  SplitJoinOp(Runner &r, Roles &R, int j) : join(j) {
+    u = R.array("u");
+    hi = R.array("uhi");
+    lo = R.array("ulo");
+    require(u->dev_dtype == DGK_FLOAT64, R.kname + ": u must be float64 on the device");
+    require(hi->dev_dtype == DGK_FLOAT32, R.kname + ": uhi must be float32 on the device");
+    same_layout(*hi, *lo, R.kname);
+    require(u->values_per_elem == hi->values_per_elem, R.kname + ": u and uhi must hold the same values per element");
+    std::vector<int64_t> c((size_t)r.npart);
+    for (int p = 0; p < r.npart; ++p) c[(size_t)p] = r.K[p] * hi->values_per_elem;
+    cnt.upload(c.data(), c.size() * sizeof(int64_t));
+    uo.upload(u->offsets.data(), sizeof(int64_t) * r.npart);
+    ho.upload(hi->offsets.data(), sizeof(int64_t) * r.npart);
+    lo_off.upload(lo->offsets.data(), sizeof(int64_t) * r.npart);
+  }
+  void launch(Runner &r, const std::vector<double> &) override {
+    SplitJoinArgs a{};
+    a.npart = r.npart;
+    a.join = join;
+    a.count = cnt.get<int64_t>();
+    a.u_off = uo.get<int64_t>();
+    a.hi_off = ho.get<int64_t>();
+    a.lo_off = lo_off.get<int64_t>();
+    a.u = reinterpret_cast<double *>(u->dptr);
+    a.hi = reinterpret_cast<float *>(hi->dptr);
+    a.lo = reinterpret_cast<float *>(lo->dptr);
+    launch_split_join(a, r.stream());
+  }
+};
+
 template <template <typename> class O, typename... A>
 std::unique_ptr<Op> typed(int dt, Runner &r, Roles &R, A... a) {
   if (dt == DGK_FLOAT64) return std::make_unique<O<double>>(r, R, a...);
@@ -382,6 +602,9 @@ std::unique_ptr<Op> make_op(Runner &r, KernelConfig &cfg, const std::string &op_
   if (name == "lserkUpdate") return typed<UpdateOp>(R.array("u")->dev_dtype, r, R, 1);
   if (name == "rhsStage") return typed<RhsOp>(R.array("u")->dev_dtype, r, R, 0);
   if (name == "rhsLF") return typed<RhsOp>(R.array("u")->dev_dtype, r, R, 1);
+  if (name == "rhsStageMixed") return std::make_unique<MixedOp>(r, R);
+  if (name == "splitState") return std::make_unique<SplitJoinOp>(r, R, 0);
+  if (name == "joinState") return std::make_unique<SplitJoinOp>(r, R, 1);
   if (name == "matmul") return typed<MatmulOp>(R.array("IN")->dev_dtype, r, R, 0);
   if (name == "matmulAdd") return typed<MatmulOp>(R.array("IN")->dev_dtype, r, R, 1);
   throw Error(DGK_ERR_NOT_FOUND, "unknown operator '" + name + "' (BuildKernel selects a precompiled operator)");

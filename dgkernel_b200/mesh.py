@@ -82,6 +82,21 @@ def face_gather_map(K, Nfaces, Nfp, Np, vmapP, EToP, node_off):
     return gmap
 
 
+def compact_faces(Kpart, node_off, face_off, Np, Nfp, gmap):
+    """Mixed-stage face connectivity from a gather map: (conn [slots, 5] int32, table [ncodes, Nfp] uint8)."""
+    K = np.ascontiguousarray(Kpart, dtype=np.int64)
+    slots = int(sum((k + 31) // 32 * 32 for k in K))
+    conn = np.zeros(max(slots, 1) * 5, dtype=np.int32)
+    table = np.zeros(256 * Nfp, dtype=np.uint8)
+    nc = C.c_int32()
+    g = np.ascontiguousarray(gmap, dtype=np.int32)
+    no = np.ascontiguousarray(node_off, dtype=np.int64)
+    fo = np.ascontiguousarray(face_off, dtype=np.int64)
+    check(lib().dgk_compact_faces(len(K), _p(K, _PI64), _p(no, _PI64), _p(fo, _PI64), Np, Nfp, _p(g, _PI32),
+                                  _p(conn, _PI32), table.ctypes.data_as(C.POINTER(C.c_uint8)), 256, C.byref(nc)))
+    return conn[:slots * 5].reshape(slots, 5), table[:nc.value * Nfp].reshape(nc.value, Nfp)
+
+
 def splitmix_uniform(seed: int, count: int) -> np.ndarray:
     out = np.zeros(count)
     check(lib().dgk_splitmix_uniform(seed, count, _p(out, _PD)))

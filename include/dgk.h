@@ -163,6 +163,16 @@ int dgk_face_connector(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const
  * at node_off[p].  This is the one-address-space form of the FaceConnector exchange. */
 int dgk_face_gather_map(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP,
                         const int64_t *EToP, int32_t npart, const int64_t *node_off, int32_t *gmap);
+/* Compact face connectivity of the mixed stage (rhsStageMixed), derived from a gather map as above: per
+ * element slot 5 int32 = the value index of each face's neighbour's first node and four packed 8-bit
+ * face-order codes, partition p's elements at slots sum_{q<p} roundup32(K[q]) + e; table_out[code*Nfp + i]
+ * = node index of face point i within the neighbour (table_cap codes of room).  gmap holds partition p's
+ * face points at face_off[p]; node_off[p] is where partition p starts in the state array.  Every gmap entry
+ * equals base + table[code][i] for its face (checked).  A derived form of the FaceConnector pick/place
+ * lists (utils/face_connector.go:143-205); the reference has no compact form. */
+int dgk_compact_faces(int32_t npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,
+                      int32_t Np, int32_t Nfp, const int32_t *gmap, int32_t *conn_out, uint8_t *table_out,
+                      int32_t table_cap, int32_t *ncodes_out);
 
 /* GPU FP64 setup (element/library/gonudg/startup3d.go:121-148, normals3d.go:11-207,
  * buildmaps3d.go:5-153) into the runner's bound arrays.  names[] lists the target binding for each of
