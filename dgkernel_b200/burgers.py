@@ -84,7 +84,7 @@ class BurgersProblem:
     residual, compact affine geometry derived from the FP64 metrics; `get("u")` joins the pair in FP64."""
 
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
-                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None):
+                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None):
         self.N, self.n, self.nslab = N, n, nslab
         self.mixed = isinstance(dtype, str) and dtype == MIXED
         self.dtype = np.dtype(np.float64) if self.mixed else np.dtype(dtype)
@@ -144,7 +144,7 @@ class BurgersProblem:
             r.BuildKernel("joinState", "joinState")
             r.ExecuteKernel("splitState")
             fixed = ["uhi", "ulo", "uhiNext", "uloNext", "resu", *GEO, *FACE, "gmap", *fixed_m, f"Bary_{sn}"]
-            op = f"rhsStageMixed(conservative={conservative})"
+            op = f"rhsStageMixed(conservative={conservative}" + (f",warps={warps})" if warps else ")")
         else:
             fixed = ["u", "uNext", "resu", *GEO, *FACE, "gmap", *fixed_m]
             op = f"rhsStage(conservative={conservative})"

@@ -27,8 +27,10 @@ int tma_tile_elems(int N);  // 0 when the order has no TMA form
 bool launch_rhs_dmma(int N, const RhsArgs<double> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info);
 int dmma_tile_elems(int N);  // 0 when the order has no such form
 
-// Mixed-precision stage (mixed.cu); returns false when the order has no such form.
-bool launch_rhs_mixed(int N, const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info);
+// Mixed-precision stage (mixed.cu) with 4, 8 or 11 consumer warps per CTA; returns false when the order or
+// the warp count has no such form.
+bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st,
+                      LaunchInfo *info);
 uint32_t mixed_slot_bytes(int N);  // 0 when the order has no such form
 template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);

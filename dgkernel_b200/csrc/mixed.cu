@@ -42,7 +42,7 @@ struct MixedCfg {
   static constexpr uint32_t GEO_B = TE * kMixedGeoWords * 4;
   static constexpr uint32_t CONN_B = TE * kMixedConnWords * 4;
   static constexpr uint32_t SLOT_B = 3 * NODE_B + GEO_B + CONN_B;  // hi, lo, resu, geometry, connectivity
-  static constexpr uint32_t DM_FLOATS = NP * 3 * NPJ;             // [i][j][r,s,t] interleaved rows
+  static constexpr uint32_t DM_FLOATS = NP * 3 * NPJ;             // [i][j/2][r,s,t][j%2] interleaved rows
   static constexpr uint32_t L_FLOATS = NP * NF;                   // LIFT rows
   static_assert(NODE_B % 16 == 0 && GEO_B % 16 == 0 && CONN_B % 16 == 0, "slot parts must stay 16-byte aligned");
   static_assert(NF % 4 == 0, "LIFT rows are read as float4");
@@ -189,7 +189,8 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
     const uint32_t codes = (uint32_t)sCon[e * kMixedConnWords + 4];
     const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
 
-    // neighbour traces uP: inside the slot from shared memory, otherwise from the previous stage's state
+    // Neighbour traces uP: inside the slot from shared memory, otherwise from the previous stage's state.  The
+    // loads are consumed only by the flux step after the volume pass, which hides their L2 latency.
     float fl[NF];
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
@@ -212,6 +213,56 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
         fl[f * NFP + i] = v;
       }
     }
+    // field minus its linear interpolant through the vertex nodes (FP64), w = u or u^2/2; pairs of columns
+    const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
+    const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
+    const double wA = cons ? 0.5 * uA * uA : uA;
+    const double dB = (cons ? 0.5 * uB * uB : uB) - wA;
+    const double dC = (cons ? 0.5 * uC * uC : uC) - wA;
+    const double dD = (cons ? 0.5 * uD * uD : uD) - wA;
+    float2 du[NPJ / 2];
+#pragma unroll
+    for (int j = 0; j < NPJ; ++j) {
+      float v = 0.f;
+      if (j < NP) {
+        const double uj = (double)hi[j] + (double)lo[j];
+        const double wj = cons ? 0.5 * uj * uj : uj;
+        v = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
+      }
+      if (j & 1)
+        du[j / 2].y = v;
+      else
+        du[j / 2].x = v;
+    }
+    // derivative of the linear part along (1,1,1): d/dr = (wB-wA)/2 and likewise for s, t
+    const float L0 = (float)(0.5 * ((double)cr * dB + (double)cs * dC + (double)ct * dD));
+
+    // Volume pass: dd_i = cr (Dr dw)_i + cs (Ds dw)_i + ct (Dt dw)_i + L0 with paired FMAs; the residual slot
+    // receives a*resu + dt*vol (the surface term is added in the next pass).
+#pragma unroll 1
+    for (int i = 0; i < NP; ++i) {
+      const float4 *Dq = reinterpret_cast<const float4 *>(sDm + i * 3 * NPJ);
+      float2 ar = make_float2(0.f, 0.f), as = ar, at = ar, br = ar, bs = ar, bt = ar;
+#pragma unroll
+      for (int g = 0; g < NPJ / 4; ++g) {
+        const float4 q0 = Dq[3 * g], q1 = Dq[3 * g + 1], q2 = Dq[3 * g + 2];
+        ar = __ffma2_rn(make_float2(q0.x, q0.y), du[2 * g], ar);
+        as = __ffma2_rn(make_float2(q0.z, q0.w), du[2 * g], as);
+        at = __ffma2_rn(make_float2(q1.x, q1.y), du[2 * g], at);
+        br = __ffma2_rn(make_float2(q1.z, q1.w), du[2 * g + 1], br);
+        bs = __ffma2_rn(make_float2(q2.x, q2.y), du[2 * g + 1], bs);
+        bt = __ffma2_rn(make_float2(q2.z, q2.w), du[2 * g + 1], bt);
+      }
+      const float ur = (ar.x + ar.y) + (br.x + br.y);
+      const float us = (as.x + as.y) + (bs.x + bs.y);
+      const float ut = (at.x + at.y) + (bt.x + bt.y);
+      const float dd = fmaf(cr, ur, fmaf(cs, us, fmaf(ct, ut, L0)));
+      const float vol = cons ? -dd : -hi[i] * dd;
+      const int o = e * NP + i;
+      const float t0 = fmaf(a, sRe[o], dt * vol);
+      if (valid) sRe[o] = t0;
+    }
+
     // Lax-Friedrichs surface term times Fscale: 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|)
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
@@ -224,67 +275,29 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
         fl[f * NFP + i] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
       }
     }
-    // field minus its linear interpolant through the vertex nodes (FP64), w = u or u^2/2
-    const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
-    const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
-    const double wA = cons ? 0.5 * uA * uA : uA;
-    const double dB = (cons ? 0.5 * uB * uB : uB) - wA;
-    const double dC = (cons ? 0.5 * uC * uC : uC) - wA;
-    const double dD = (cons ? 0.5 * uD * uD : uD) - wA;
-    float du[NPJ];
-#pragma unroll
-    for (int j = 0; j < NPJ; ++j) {
-      if (j < NP) {
-        const double uj = (double)hi[j] + (double)lo[j];
-        const double wj = cons ? 0.5 * uj * uj : uj;
-        du[j] = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
-      } else {
-        du[j] = 0.f;
-      }
-    }
-    // derivative of the linear part along (1,1,1): d/dr = (wB-wA)/2 and likewise for s, t
-    const float L0 = (float)(0.5 * ((double)cr * dB + (double)cs * dC + (double)ct * dD));
     __syncwarp();  // every lane has read the slot's traces before any lane overwrites its own state
 
+    // Surface pass: LIFT row times the flux (paired FMAs), then the stage update in FP64, split into hi + lo.
     const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
 #pragma unroll 1
     for (int i = 0; i < NP; ++i) {
-      const float4 *Dq = reinterpret_cast<const float4 *>(sDm + i * 3 * NPJ);
-      float r0 = 0.f, s0 = 0.f, t0 = 0.f, r1 = 0.f, s1 = 0.f, t1 = 0.f;
-#pragma unroll
-      for (int g = 0; g < NPJ / 4; ++g) {
-        const float4 q0 = Dq[3 * g], q1 = Dq[3 * g + 1], q2 = Dq[3 * g + 2];
-        const float d0 = du[4 * g], d1 = du[4 * g + 1], d2 = du[4 * g + 2], d3 = du[4 * g + 3];
-        r0 = fmaf(q0.x, d0, r0);
-        s0 = fmaf(q0.y, d0, s0);
-        t0 = fmaf(q0.z, d0, t0);
-        r1 = fmaf(q0.w, d1, r1);
-        s1 = fmaf(q1.x, d1, s1);
-        t1 = fmaf(q1.y, d1, t1);
-        r0 = fmaf(q1.z, d2, r0);
-        s0 = fmaf(q1.w, d2, s0);
-        t0 = fmaf(q2.x, d2, t0);
-        r1 = fmaf(q2.y, d3, r1);
-        s1 = fmaf(q2.z, d3, s1);
-        t1 = fmaf(q2.w, d3, t1);
-      }
-      const float dd = fmaf(cr, r0 + r1, fmaf(cs, s0 + s1, fmaf(ct, t0 + t1, L0)));
       const float4 *Lq = reinterpret_cast<const float4 *>(sL + i * NF);
-      float l0 = 0.f, l1 = 0.f;
+      float2 l0 = make_float2(0.f, 0.f), l1 = l0, l2 = l0, l3 = l0;
 #pragma unroll
       for (int g = 0; g < NF / 4; ++g) {
-        const float4 q = Lq[g];
-        l0 = fmaf(q.x, fl[4 * g], l0);
-        l1 = fmaf(q.y, fl[4 * g + 1], l1);
-        l0 = fmaf(q.z, fl[4 * g + 2], l0);
-        l1 = fmaf(q.w, fl[4 * g + 3], l1);
+        const float4 m = Lq[g];
+        if (g & 1) {
+          l2 = __ffma2_rn(make_float2(m.x, m.y), make_float2(fl[4 * g], fl[4 * g + 1]), l2);
+          l3 = __ffma2_rn(make_float2(m.z, m.w), make_float2(fl[4 * g + 2], fl[4 * g + 3]), l3);
+        } else {
+          l0 = __ffma2_rn(make_float2(m.x, m.y), make_float2(fl[4 * g], fl[4 * g + 1]), l0);
+          l1 = __ffma2_rn(make_float2(m.z, m.w), make_float2(fl[4 * g + 2], fl[4 * g + 3]), l1);
+        }
       }
-      const float hi_i = hi[i];
-      const float vol = cons ? -dd : -hi_i * dd;
-      const float rhs = vol + (l0 + l1);
+      const float lift = ((l0.x + l0.y) + (l1.x + l1.y)) + ((l2.x + l2.y) + (l3.x + l3.y));
       const int o = e * NP + i;
-      const float rn = fmaf(a, sRe[o], dt * rhs);
-      const double un = ((double)hi_i + (double)lo[i]) + b * (double)rn;
+      const float rn = fmaf(dt, lift, sRe[o]);
+      const double un = ((double)hi[i] + (double)lo[i]) + b * (double)rn;
       const float hn = __double2float_rn(un);
       const float ln = __double2float_rn(un - (double)hn);
       if (valid) {
@@ -317,20 +330,16 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
 
 namespace {
 
-constexpr int kMixedConsumerWarps = 8;
 constexpr uint32_t kSmemBudget = 227 * 1024;
 
-template <int N>
+template <int N, int CW>
 bool launch_mixed_n(const MixedArgs &A0, int num_sms, cudaStream_t st, LaunchInfo *info) {
   using C = MixedCfg<N>;
-  constexpr int CW = kMixedConsumerWarps;
   MixedArgs A = A0;
-  const MixedSmem fixed = mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, 0, A.ncodes);
   int ns = 0;
-  while (ns < 16 && mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, ns + 1, A.ncodes).total <=
+  while (ns < 24 && mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, ns + 1, A.ncodes).total <=
                         kSmemBudget)
     ++ns;
-  (void)fixed;
   if (ns < 2) return false;
   A.ns = ns;
   const uint32_t smem = mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, ns, A.ncodes).total;
@@ -342,6 +351,16 @@ bool launch_mixed_n(const MixedArgs &A0, int num_sms, cudaStream_t st, LaunchInf
   cuda_check(cudaGetLastError(), "rhs_stage_mixed_kernel launch");
   if (info) *info = LaunchInfo{grid, 32 * (CW + 1), (int)smem, 1};
   return true;
+}
+
+template <int N>
+bool launch_mixed_cw(const MixedArgs &A, int cw, int num_sms, cudaStream_t st, LaunchInfo *info) {
+  switch (cw) {
+    case 4: return launch_mixed_n<N, 4>(A, num_sms, st, info);
+    case 8: return launch_mixed_n<N, 8>(A, num_sms, st, info);
+    case 11: return launch_mixed_n<N, 11>(A, num_sms, st, info);
+    default: return false;
+  }
 }
 
 // Compact per-element geometry: cr, cs, ct and g_f = Fscale_f (nx+ny+nz)_f, with an affinity check.
@@ -416,13 +435,14 @@ __global__ void split_join_kernel(SplitJoinArgs a) {
 
 }  // namespace
 
-bool launch_rhs_mixed(int N, const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info) {
+bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st,
+                      LaunchInfo *info) {
   switch (N) {
-    case 1: return launch_mixed_n<1>(A, num_sms, st, info);
-    case 2: return launch_mixed_n<2>(A, num_sms, st, info);
-    case 3: return launch_mixed_n<3>(A, num_sms, st, info);
-    case 4: return launch_mixed_n<4>(A, num_sms, st, info);
-    case 5: return launch_mixed_n<5>(A, num_sms, st, info);
+    case 1: return launch_mixed_cw<1>(A, consumer_warps, num_sms, st, info);
+    case 2: return launch_mixed_cw<2>(A, consumer_warps, num_sms, st, info);
+    case 3: return launch_mixed_cw<3>(A, consumer_warps, num_sms, st, info);
+    case 4: return launch_mixed_cw<4>(A, consumer_warps, num_sms, st, info);
+    case 5: return launch_mixed_cw<5>(A, consumer_warps, num_sms, st, info);
     default: return false;
   }
 }

@@ -370,7 +370,7 @@ struct MatmulOp : Op {
 // nz, Fscale (float64 or float32, read at build time only); gmap (int32, value indices into uhi's layout);
 // matrices Dr, Ds, Dt, LIFT, Fmask and Bary (Np x 4 barycentric coordinates of the nodes).
 struct MixedOp : Op {
-  int N = 0, ntiles = 0, conservative = 0, ncodes = 0;
+  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
   DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask;
   LaunchInfo info;
@@ -414,6 +414,8 @@ struct MixedOp : Op {
     static const char *gn[9] = {"Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz"};
     static const char *fn[4] = {"nx", "ny", "nz", "Fscale"};
     conservative = R.flag("conservative", 0);
+    warps = R.flag("warps", 11);
+    require(warps == 4 || warps == 8 || warps == 11, R.kname + ": warps must be 4, 8 or 11");
     uhi = R.array("uhi");
     ulo = R.array("ulo");
     uhin = R.array("uhiNext");
@@ -472,15 +474,15 @@ struct MixedOp : Op {
     if (cf.table.empty()) cf.table.assign((size_t)nfp, 0);
     conn.upload(cf.conn.data(), std::max<size_t>(cf.conn.size(), 1) * sizeof(int32_t));
     ftab.upload(cf.table.data(), cf.table.size());
-    // Dr, Ds, Dt interleaved per column ([i][j][r,s,t]), columns padded to a multiple of 4 with zeros
+    // Dr, Ds, Dt interleaved by column pairs ([i][j/2][r,s,t][j%2]), columns padded to a multiple of 4 with
+    // zeros: one row's pair of columns feeds three paired FMAs
     const int npj = ((int)np + 3) & ~3;
     std::vector<float> d((size_t)(np * npj * 3), 0.f);
+    const Binding *D3[3] = {Dr, Ds, Dt};
     for (int64_t i = 0; i < np; ++i)
-      for (int64_t j = 0; j < np; ++j) {
-        d[(size_t)((i * npj + j) * 3 + 0)] = (float)Dr->mat[(size_t)(i * np + j)];
-        d[(size_t)((i * npj + j) * 3 + 1)] = (float)Ds->mat[(size_t)(i * np + j)];
-        d[(size_t)((i * npj + j) * 3 + 2)] = (float)Dt->mat[(size_t)(i * np + j)];
-      }
+      for (int64_t j = 0; j < np; ++j)
+        for (int c = 0; c < 3; ++c)
+          d[(size_t)(i * 3 * npj + (j / 2) * 6 + c * 2 + (j % 2))] = (float)D3[c]->mat[(size_t)(i * np + j)];
     dm.upload(d.data(), d.size() * sizeof(float));
     auto lt = cast<float>(L->mat);
     lift.upload(lt.data(), lt.size() * sizeof(float));
@@ -540,7 +542,7 @@ struct MixedOp : Op {
     A.dt = (float)s[2];
     A.conservative = conservative;
     A.status = r.status_word();
-    if (!launch_rhs_mixed(N, A, r.num_sms, r.stream(), &info))
+    if (!launch_rhs_mixed(N, A, warps, r.num_sms, r.stream(), &info))
       throw Error(DGK_ERR_UNSUPPORTED, "mixed stage: no launch shape fits shared memory for this order");
     std::swap(uhi->dptr, uhin->dptr);  // "uhi"/"ulo" always name the newest state
     std::swap(ulo->dptr, ulon->dptr);
