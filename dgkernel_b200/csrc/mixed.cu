@@ -189,30 +189,6 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
     const uint32_t codes = (uint32_t)sCon[e * kMixedConnWords + 4];
     const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
 
-    // Neighbour traces uP: inside the slot from shared memory, otherwise from the previous stage's state.  The
-    // loads are consumed only by the flux step after the volume pass, which hides their L2 latency.
-    float fl[NF];
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      const int64_t nb = sCon[e * kMixedConnWords + f];
-      const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
-      const uint8_t *ft = sFt + cd * NFP;
-      const bool ins = (uint64_t)(nb - slot0) < (uint64_t)slotn;
-#pragma unroll
-      for (int i = 0; i < NFP; ++i) {
-        const int64_t idx = nb + ft[i];
-        float v;
-        if (ins) {
-          v = sHi[idx - slot0];
-        } else if (valid && (uint64_t)idx < (uint64_t)A.n_u_values) {
-          v = __ldg(A.uhi_in + idx);
-        } else {
-          v = hi[sFm[f * NFP + i]];
-          if (valid) atomicExch(A.status, kStatusBadGather);
-        }
-        fl[f * NFP + i] = v;
-      }
-    }
     // field minus its linear interpolant through the vertex nodes (FP64), w = u or u^2/2; pairs of columns
     const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
     const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
@@ -263,6 +239,27 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
       if (valid) sRe[o] = t0;
     }
 
+    // Neighbour traces uP: inside the slot from shared memory, otherwise from the previous stage's state, read
+    // through one generic address per point (no divergent branch between the two memories).  They are loaded
+    // after the volume pass so that the pass runs with the fewest live registers.
+    float fl[NF];
+    bool bad = false;
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const int64_t nb = sCon[e * kMixedConnWords + f];
+      const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
+      const uint8_t *ft = sFt + cd * NFP;
+      const bool ins = (uint64_t)(nb - slot0) < (uint64_t)slotn;
+#pragma unroll
+      for (int i = 0; i < NFP; ++i) {
+        const int64_t idx = nb + ft[i];
+        const bool okg = (uint64_t)idx < (uint64_t)A.n_u_values;
+        bad |= valid && !ins && !okg;
+        const float *src = ins ? sHi + (idx - slot0) : (okg ? A.uhi_in + idx : hi + sFm[f * NFP + i]);
+        fl[f * NFP + i] = *src;
+      }
+    }
+    if (bad) atomicExch(A.status, kStatusBadGather);
     // Lax-Friedrichs surface term times Fscale: 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|)
 #pragma unroll
     for (int f = 0; f < 4; ++f) {
