@@ -48,6 +48,10 @@ SIGNATURES = {
     "dgk_ti_connect3d": [_I64, _PI64, _PI64, _PI64],
     "dgk_face_connector": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI64, _PI64],
     "dgk_face_gather_map": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI32],
+    "dgk_init_field_parts": [_P, _S, _S, _S, _S, _D, _I32, _PD],
+    "dgk_capture_graph": [_P, _S, _I32, _I32, _PD, C.POINTER(_P)],
+    "dgk_graph_launch": [_P, _I32],
+    "dgk_graph_free": [_P],
     "dgk_compact_faces": [_I32, _PI64, _PI64, _PI64, _I32, _I32, _PI32, _PI32, C.POINTER(C.c_uint8), _I32, _PI32],
     "dgk_setup_geometry": [_P, _P, _I64, _PD, _PD, _PD, _PI64, _PI64, _PI64, _D, C.POINTER(_S), _PD],
     "dgk_init_field": [_P, _S, _S, _S, _S, _I32, _D, _D, _I32, _PD],

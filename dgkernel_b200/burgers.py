@@ -76,27 +76,51 @@ def bary_matrix(el) -> np.ndarray:
 MIXED = "mixed"
 
 
-class BurgersProblem:
-    """Device-resident Burgers problem of order N on an n^3 x 6 Kuhn mesh with nslab x-slab partitions.
+def ensemble_sizes(count: int = 256, lo: int = 6, hi: int = 24, seed: int = DEFAULT_SEED):
+    """Cube counts per axis of a seeded batch of instances: n_i uniform on {lo..hi} from a splitmix64 stream."""
+    u = M.splitmix_uniform(seed, count)
+    return [lo + int(math.floor(v * (hi - lo + 1))) for v in u]
+
+
+def _concat_meshes(sizes):
+    """Independent periodic n^3 x 6 Kuhn meshes side by side: vertex and element ids offset per instance,
+    EToP = instance index, so every instance is one partition with no face shared with another."""
+    VX, VY, VZ, EToV, EToE, EToF, EToP = [], [], [], [], [], [], []
+    voff = eoff = 0
+    for i, n in enumerate(sizes):
+        vx, vy, vz, etov, etovp, _ = M.kuhn_mesh(int(n), 1)
+        etoe, etof = M.ti_connect3d(etovp)
+        VX.append(vx), VY.append(vy), VZ.append(vz)
+        EToV.append(etov + voff)
+        EToE.append(etoe + eoff)
+        EToF.append(etof)
+        EToP.append(np.full(etov.shape[0], i, dtype=np.int64))
+        voff += len(vx)
+        eoff += etov.shape[0]
+    cat = lambda xs: np.ascontiguousarray(np.concatenate(xs))
+    return cat(VX), cat(VY), cat(VZ), cat(EToV), cat(EToE), cat(EToF), cat(EToP)
+
+
+class _TetBurgers:
+    """Assembly shared by the single-mesh problem and the batch of instances: bindings for state, geometry,
+    face data and reference matrices; FP64 geometry, normals and periodic VmapP computed on the GPU; the
+    FaceConnector exchange fused into a gather map; one stage operator.
 
     dtype float64 / float32: the plain stage (`rhsStage`) with state, metrics and face data in that type.
     dtype "mixed": the mixed-precision stage (`rhsStageMixed`): compensated FP32 state uhi + ulo, FP32
     residual, compact affine geometry derived from the FP64 metrics; `get("u")` joins the pair in FP64."""
 
-    def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
-                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None):
-        self.N, self.n, self.nslab = N, n, nslab
+    def _assemble(self, N, VX, VY, VZ, EToV, EToE, EToF, EToP, Kpart, dtype, stream):
+        self.N = N
         self.mixed = isinstance(dtype, str) and dtype == MIXED
         self.dtype = np.dtype(np.float64) if self.mixed else np.dtype(dtype)
         dt_code = Float64 if self.dtype == np.float64 else Float32
         el = self.el = Element(N)
         Np, Nfp = el.Np, el.Nfp
         NF = 4 * Nfp
-        VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)
         self.EToV, self.EToP = EToV, EToP
-        EToE, EToF = M.ti_connect3d(EToVp)
         K = self.K = EToV.shape[0]
-        self.Kpart = [K // nslab] * nslab
+        self.Kpart = list(Kpart)
         r = self.runner = Runner(Config(K=self.Kpart), stream=stream)
         sn = el.ShortName
         state = ("u", "X", "Y", "Z") if self.mixed else ("u", "uNext", "resu", "X", "Y", "Z")
@@ -117,8 +141,6 @@ class BurgersProblem:
         names = ["X", "Y", "Z", *GEO, None, "nx", "ny", "nz", None, "Fscale", None, "vmapP"]
         carr = (C.c_char_p * 20)(*[None if v is None else v.encode() for v in names])
         hmin = C.c_double()
-        _pd = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
-        _pi = lambda a: a.ctypes.data_as(C.POINTER(C.c_int64))
         check(lib().dgk_setup_geometry(r._h, el._h, len(VX), _pd(VX), _pd(VY), _pd(VZ), _pi(EToV), _pi(EToE),
                                        _pi(EToF), 2.0, carr, C.byref(hmin)), r._h)
         self.hmin = hmin.value
@@ -128,14 +150,10 @@ class BurgersProblem:
         self.node_off = r.GetOffsets("uhi" if self.mixed else "u")
         self.gmap = M.face_gather_map(K, 4, Nfp, Np, self.vmapP, EToP, self.node_off)
         r.CopyToDevice("gmap", self.gmap)
-        # initial condition
-        if u0_host is not None:
-            r.CopyToDevice("u", np.ascontiguousarray(u0_host, dtype=self.dtype).reshape(-1))
-        else:
-            kinds = {"sine": (0, 0.0, 0.5), "shock": (0, 0.5, 1.0), "smooth": (1, 0.5, 0.25), "modes": (2, 0.5, 0.0)}
-            kind, mean, amp = kinds[u0]
-            modes = random_modes(seed) if kind == 2 else np.zeros((0, 5))
-            check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, len(modes), _pd(modes)), r._h)
+
+    def _finish(self, cfl, conservative, warps=None, ring=None):
+        r, el = self.runner, self.el
+        sn = el.ShortName
         fixed_m = [f"Dr_{sn}", f"Ds_{sn}", f"Dt_{sn}", f"LIFT_{sn}", "Fmask"]
         if self.mixed:
             r.ConfigureKernel("splitState", r.Param("u"), r.Param("uhi"), r.Param("ulo"))
@@ -144,15 +162,30 @@ class BurgersProblem:
             r.BuildKernel("joinState", "joinState")
             r.ExecuteKernel("splitState")
             fixed = ["uhi", "ulo", "uhiNext", "uloNext", "resu", *GEO, *FACE, "gmap", *fixed_m, f"Bary_{sn}"]
-            op = f"rhsStageMixed(conservative={conservative}" + (f",warps={warps})" if warps else ")")
         else:
             fixed = ["u", "uNext", "resu", *GEO, *FACE, "gmap", *fixed_m]
-            op = f"rhsStage(conservative={conservative})"
+        self.conservative = conservative
         self.u0 = self.get("u")
         self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))
         r.ConfigureKernel("rhsStage", *[r.Param(p) for p in fixed], r.Param("a"), r.Param("b"), r.Param("dt"))
-        r.BuildKernel(op, "rhsStage")
         self.stage = 0
+        self.build_stage(warps=warps, ring=ring)
+
+    def op_id(self, warps=None, ring=None) -> str:
+        """Operator id of the stage kernel, with the launch shape (mixed stage) when given."""
+        if not self.mixed:
+            return f"rhsStage(conservative={self.conservative})"
+        args = [f"conservative={self.conservative}"]
+        if warps:
+            args.append(f"warps={warps}")
+        if ring:
+            args.append(f"ring={ring}")
+        return "rhsStageMixed(" + ",".join(args) + ")"
+
+    def build_stage(self, warps=None, ring=None):
+        """(Re)build the stage operator, optionally with a given launch shape."""
+        self.shape = {"warps": warps, "ring": ring}
+        self.runner.BuildKernel(self.op_id(warps, ring), "rhsStage")
 
     @property
     def dofs(self) -> int:
@@ -181,5 +214,74 @@ class BurgersProblem:
             self.runner.ExecuteKernel("rhsStage", RK4A[s], RK4B[s], self.dt)
             self.stage += 1
 
+    def capture_steps(self, nsteps: int = 2):
+        """CUDA graph of `nsteps` whole LSERK4 steps (5 stages each; nsteps even so that the ping-pong state
+        returns to its buffers); replay with `run_graph`.  Must start at a step boundary."""
+        if self.stage % 5 or nsteps < 2 or nsteps % 2:
+            raise ValueError("capture whole steps, an even number of them, from a step boundary")
+        rows = [(RK4A[s % 5], RK4B[s % 5], self.dt) for s in range(5 * nsteps)]
+        g = self.runner.CaptureGraph("rhsStage", rows)
+        g.steps = nsteps
+        return g
+
+    def run_graph(self, graph, repeats: int = 1):
+        graph.Launch(repeats)
+        self.stage += 5 * graph.steps * repeats
+
     def free(self):
         self.runner.Free()
+
+
+class BurgersProblem(_TetBurgers):
+    """Device-resident Burgers problem of order N on one periodic n^3 x 6 Kuhn mesh with nslab x-slab
+    partitions (u0: "sine", "shock", "smooth" or "modes"; dtype float64, float32 or "mixed")."""
+
+    def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
+                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None):
+        self.n, self.nslab = n, nslab
+        VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)
+        EToE, EToF = M.ti_connect3d(EToVp)
+        K = EToV.shape[0]
+        self._assemble(N, VX, VY, VZ, EToV, EToE, EToF, EToP, [K // nslab] * nslab, dtype, stream)
+        r = self.runner
+        if u0_host is not None:
+            r.CopyToDevice("u", np.ascontiguousarray(u0_host, dtype=self.dtype).reshape(-1))
+        else:
+            kinds = {"sine": (0, 0.0, 0.5), "shock": (0, 0.5, 1.0), "smooth": (1, 0.5, 0.25), "modes": (2, 0.5, 0.0)}
+            kind, mean, amp = kinds[u0]
+            modes = random_modes(seed) if kind == 2 else np.zeros((0, 5))
+            check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, len(modes), _pd(modes)), r._h)
+        self._finish(cfl, conservative, warps, ring)
+
+
+class BurgersEnsemble(_TetBurgers):
+    """A batch of independent Burgers instances of order N, instance i on its own periodic n_i^3 x 6 Kuhn mesh
+    (uneven K_i = 6 n_i^3), all in one runner with one partition per instance, so that one stage launch (and
+    one persistent grid) advances every instance.  Instance i starts from 0.5 + 8 random modes drawn with
+    seed + i; all instances share one time step, the CFL step of the most restrictive one."""
+
+    def __init__(self, N: int, sizes, dtype=MIXED, seed: int = DEFAULT_SEED, cfl: float = 0.3, conservative: int = 0,
+                 stream=None, warps=None, ring=None):
+        self.sizes = [int(n) for n in sizes]
+        VX, VY, VZ, EToV, EToE, EToF, EToP = _concat_meshes(self.sizes)
+        Kpart = [6 * n ** 3 for n in self.sizes]
+        self._assemble(N, VX, VY, VZ, EToV, EToE, EToF, EToP, Kpart, dtype, stream)
+        r = self.runner
+        modes = np.ascontiguousarray(np.concatenate([random_modes(seed + i) for i in range(len(self.sizes))]))
+        check(lib().dgk_init_field_parts(r._h, b"u", b"X", b"Y", b"Z", 0.5, 8, _pd(modes)), r._h)
+        self.modes = modes.reshape(len(self.sizes), 8, 5)
+        self._finish(cfl, conservative, warps, ring)
+
+    def instance(self, i: int, u: np.ndarray = None) -> np.ndarray:
+        """Instance i's nodal values (FP64, element-contiguous) from a packed state (default: the current one)."""
+        u = self.get("u") if u is None else u
+        off = int(sum(self.Kpart[:i])) * self.el.Np
+        return u[off:off + self.Kpart[i] * self.el.Np]
+
+
+def _pd(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _pi(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))

@@ -1,6 +1,7 @@
 // extern "C" entry points of libdgk.so (declared in include/dgk.h).  Every call converts C++ exceptions
 // into a status code plus a retrievable message; nothing throws across the ABI.
 #include <cstring>
+#include <memory>
 #include <string>
 
 #include "element.hpp"
@@ -15,6 +16,11 @@ struct dgk_runner {
 struct dgk_element {
   dgk::RefElement impl;
   explicit dgk_element(int N) : impl(N) {}
+};
+struct dgk_graph {
+  dgk_runner *r = nullptr;
+  dgk::Runner::Graph *g = nullptr;
+  ~dgk_graph() { delete g; }
 };
 
 namespace {
@@ -341,33 +347,71 @@ int dgk_setup_geometry(dgk_runner *r, const dgk_element *e, int64_t nverts, cons
   });
 }
 
+namespace {
+// Evaluate the initial field per partition; modes_per_part selects one mode set per partition.
+void init_field(dgk_runner *r, const char *name, const char *xn, const char *yn, const char *zn, int32_t kind,
+                double mean, double amp, int32_t nmodes, const double *modes, bool modes_per_part) {
+  dgk::Runner &R = r->impl;
+  dgk::Binding &u = R.binding(name), &X = R.binding(xn), &Y = R.binding(yn), &Z = R.binding(zn);
+  for (dgk::Binding *b : {&X, &Y, &Z})
+    if (b->dev_dtype != u.dev_dtype || b->offsets != u.offsets)
+      throw dgk::Error(DGK_ERR_INVALID, "coordinates must share the field's type and layout");
+  if (nmodes < 0 || (nmodes > 0 && !modes)) throw dgk::Error(DGK_ERR_INVALID, "modes missing");
+  const int64_t rows = (int64_t)nmodes * (modes_per_part ? R.npart : 1);
+  double *dm = nullptr;
+  if (rows > 0) {
+    dgk::cuda_check(cudaMalloc(reinterpret_cast<void **>(&dm), sizeof(double) * 5 * rows), "cudaMalloc(modes)");
+    dgk::cuda_check(cudaMemcpy(dm, modes, sizeof(double) * 5 * rows, cudaMemcpyHostToDevice), "modes");
+  }
+  for (int p = 0; p < R.npart; ++p) {
+    const int64_t o = u.offsets[p], n = R.K[p] * u.values_per_elem;
+    const double *mp = dm ? dm + (modes_per_part ? (int64_t)5 * nmodes * p : 0) : nullptr;
+    if (u.dev_dtype == DGK_FLOAT64)
+      dgk::launch_field<double>(reinterpret_cast<double *>(u.dptr) + o, reinterpret_cast<double *>(X.dptr) + o,
+                                reinterpret_cast<double *>(Y.dptr) + o, reinterpret_cast<double *>(Z.dptr) + o, n, kind,
+                                mean, amp, mp, nmodes, R.stream());
+    else
+      dgk::launch_field<float>(reinterpret_cast<float *>(u.dptr) + o, reinterpret_cast<float *>(X.dptr) + o,
+                               reinterpret_cast<float *>(Y.dptr) + o, reinterpret_cast<float *>(Z.dptr) + o, n, kind,
+                               mean, amp, mp, nmodes, R.stream());
+  }
+  dgk::cuda_check(cudaStreamSynchronize(R.stream()), "sync");
+  if (dm) cudaFree(dm);
+}
+}  // namespace
+
 int dgk_init_field(dgk_runner *r, const char *name, const char *xn, const char *yn, const char *zn, int32_t kind,
                    double mean, double amp, int32_t nmodes, const double *modes) {
+  return guard(r, [&] { init_field(r, name, xn, yn, zn, kind, mean, amp, nmodes, modes, false); });
+}
+
+int dgk_init_field_parts(dgk_runner *r, const char *name, const char *xn, const char *yn, const char *zn,
+                         double mean, int32_t nmodes, const double *modes) {
+  return guard(r, [&] { init_field(r, name, xn, yn, zn, 2, mean, 0.0, nmodes, modes, true); });
+}
+
+int dgk_capture_graph(dgk_runner *r, const char *kernel_name, int32_t nlaunch, int32_t nscalars,
+                      const double *scalars, dgk_graph **out) {
   return guard(r, [&] {
-    dgk::Runner &R = r->impl;
-    dgk::Binding &u = R.binding(name), &X = R.binding(xn), &Y = R.binding(yn), &Z = R.binding(zn);
-    for (dgk::Binding *b : {&X, &Y, &Z})
-      if (b->dev_dtype != u.dev_dtype || b->offsets != u.offsets)
-        throw dgk::Error(DGK_ERR_INVALID, "coordinates must share the field's type and layout");
-    double *dm = nullptr;
-    if (nmodes > 0) {
-      dgk::cuda_check(cudaMalloc(reinterpret_cast<void **>(&dm), sizeof(double) * 5 * nmodes), "cudaMalloc(modes)");
-      dgk::cuda_check(cudaMemcpy(dm, modes, sizeof(double) * 5 * nmodes, cudaMemcpyHostToDevice), "modes");
-    }
-    for (int p = 0; p < R.npart; ++p) {
-      const int64_t o = u.offsets[p], n = R.K[p] * u.values_per_elem;
-      if (u.dev_dtype == DGK_FLOAT64)
-        dgk::launch_field<double>(reinterpret_cast<double *>(u.dptr) + o, reinterpret_cast<double *>(X.dptr) + o,
-                                  reinterpret_cast<double *>(Y.dptr) + o, reinterpret_cast<double *>(Z.dptr) + o, n, kind,
-                                  mean, amp, dm, nmodes, R.stream());
-      else
-        dgk::launch_field<float>(reinterpret_cast<float *>(u.dptr) + o, reinterpret_cast<float *>(X.dptr) + o,
-                                 reinterpret_cast<float *>(Y.dptr) + o, reinterpret_cast<float *>(Z.dptr) + o, n, kind,
-                                 mean, amp, dm, nmodes, R.stream());
-    }
-    dgk::cuda_check(cudaStreamSynchronize(R.stream()), "sync");
-    if (dm) cudaFree(dm);
+    if (!r || !out) throw dgk::Error(DGK_ERR_INVALID, "null runner or output");
+    std::unique_ptr<dgk_graph> h(new dgk_graph);
+    h->r = r;
+    h->g = r->impl.capture_graph(kernel_name, nlaunch, nscalars, scalars);
+    *out = h.release();
   });
+}
+
+int dgk_graph_launch(dgk_graph *g, int32_t repeats) {
+  if (!g) {
+    g_error = "null graph";
+    return DGK_ERR_INVALID;
+  }
+  return guard(g->r, [&] { g->r->impl.launch_graph(*g->g, repeats); });
+}
+
+int dgk_graph_free(dgk_graph *g) {
+  delete g;
+  return DGK_OK;
 }
 
 }  // extern "C"

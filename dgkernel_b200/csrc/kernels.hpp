@@ -27,10 +27,11 @@ int tma_tile_elems(int N);  // 0 when the order has no TMA form
 bool launch_rhs_dmma(int N, const RhsArgs<double> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info);
 int dmma_tile_elems(int N);  // 0 when the order has no such form
 
-// Mixed-precision stage (mixed.cu) with 4, 8 or 11 consumer warps per CTA; returns false when the order or
-// the warp count has no such form.
-bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st,
+// Mixed-precision stage (mixed.cu) with 4, 8 or 11 consumer warps per CTA and at most ring_max ring slots
+// (0: as many as shared memory holds); returns false when the order or the warp count has no such form.
+bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int ring_max, int num_sms, cudaStream_t st,
                       LaunchInfo *info);
+void prepare_rhs_mixed(int N, int consumer_warps);  // attributes, before any stream capture
 uint32_t mixed_slot_bytes(int N);  // 0 when the order has no such form
 template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);

@@ -50,7 +50,7 @@ struct MixedCfg {
 
 // Shared-memory layout of the kernel (host and device agree through this function).
 struct MixedSmem {
-  uint32_t ring, dm, lift, bary, bars, ftab, fmask, misc, total;
+  uint32_t ring, dm, lift, bary, bars, tags, ftab, fmask, misc, total;
 };
 __host__ __device__ inline MixedSmem mixed_smem(uint32_t slot_b, uint32_t dm_floats, uint32_t l_floats, int np,
                                                int nfp, int ns, int ncodes) {
@@ -60,7 +60,8 @@ __host__ __device__ inline MixedSmem mixed_smem(uint32_t slot_b, uint32_t dm_flo
   m.lift = m.dm + dm_floats * 4;
   m.bary = m.lift + l_floats * 4;
   m.bars = m.bary + (uint32_t)np * 3 * 8;
-  m.ftab = m.bars + 2u * (uint32_t)ns * 8;
+  m.tags = m.bars + 2u * (uint32_t)ns * 8;
+  m.ftab = m.tags + round16(4u * (uint32_t)ns);
   m.fmask = m.ftab + round16((uint32_t)(ncodes * nfp));
   m.misc = m.fmask + round16((uint32_t)(4 * nfp));
   m.total = m.misc + 32;
@@ -103,6 +104,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
   uint8_t *sFt = sm + L.ftab;
   uint8_t *sFm = sm + L.fmask;
   int *sMisc = reinterpret_cast<int *>(sm + L.misc);  // [0..3] vertex nodes A..D, [4] abort flag
+  int *sTag = reinterpret_cast<int *>(sm + L.tags);    // local tile index last issued into each slot
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int G = gridDim.x;
 
@@ -115,6 +117,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
   if (tid == 0) {
     sMisc[4] = 0;
     for (int s = 0; s < NS; ++s) {
+      sTag[s] = -1;
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -138,6 +141,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
           bad = true;
           break;
         }
+        *reinterpret_cast<volatile int *>(&sTag[s]) = k;  // fill k/NS of slot s is issued (k-NS was consumed)
         issue_slot<N>(A, A.tiles[t], ring + (size_t)s * C::SLOT_B, &full[s]);
       }
       if (bad) {
@@ -162,7 +166,16 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_mixed_kernel(const
     const int t = blockIdx.x + k * G;
     if (t >= A.ntiles) break;
     const int s = k % NS;
-    bool ok = mbar_wait_bounded(&full[s], (uint32_t)(k / NS) & 1u, kSpinLimit);
+    // Warps own fixed tiles but share the ring, so a warp can reach tile k while the slot still waits for an
+    // earlier occupant; its parity wait is unambiguous only once the fill before k's has completed, which the
+    // producer guarantees by the time it tags the slot with k.
+    bool ok = false;
+    for (uint32_t it = 0; it < kSpinLimit; ++it)
+      if (vload(&sTag[s]) == k || vload(&sMisc[4])) {
+        ok = vload(&sTag[s]) == k;
+        break;
+      }
+    ok = ok && mbar_wait_bounded(&full[s], (uint32_t)(k / NS) & 1u, kSpinLimit);
     ok = __all_sync(0xffffffffu, ok) && !vload(&sMisc[4]);
     if (!ok) {
       if (lane == 0) {
@@ -329,20 +342,34 @@ namespace {
 
 constexpr uint32_t kSmemBudget = 227 * 1024;
 
+// The shared-memory opt-in of one instantiation, raised to the budget once per device (so that launches recorded
+// by a stream capture need no attribute call).
 template <int N, int CW>
-bool launch_mixed_n(const MixedArgs &A0, int num_sms, cudaStream_t st, LaunchInfo *info) {
+void mixed_attr() {
+  static bool done[64] = {};
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev >= 0 && dev < 64 && done[dev]) return;
+  cuda_check(cudaFuncSetAttribute(rhs_stage_mixed_kernel<N, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmemBudget),
+             "mixed kernel smem attribute");
+  if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+template <int N, int CW>
+bool launch_mixed_n(const MixedArgs &A0, int ring_max, int num_sms, cudaStream_t st, LaunchInfo *info) {
   using C = MixedCfg<N>;
   MixedArgs A = A0;
   int ns = 0;
-  while (ns < 24 && mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, ns + 1, A.ncodes).total <=
-                        kSmemBudget)
+  const int cap = ring_max > 0 ? std::min(ring_max, 24) : 24;
+  while (ns < cap && mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, ns + 1, A.ncodes).total <=
+                         kSmemBudget)
     ++ns;
   if (ns < 2) return false;
   A.ns = ns;
   const uint32_t smem = mixed_smem(C::SLOT_B, C::DM_FLOATS, C::L_FLOATS, C::NP, C::NFP, ns, A.ncodes).total;
   auto kern = rhs_stage_mixed_kernel<N, CW>;
-  cuda_check(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-             "mixed kernel smem attribute");
+  mixed_attr<N, CW>();
   const int grid = std::max(1, std::min(num_sms, A.ntiles));
   kern<<<grid, 32 * (CW + 1), smem, st>>>(A);
   cuda_check(cudaGetLastError(), "rhs_stage_mixed_kernel launch");
@@ -351,11 +378,18 @@ bool launch_mixed_n(const MixedArgs &A0, int num_sms, cudaStream_t st, LaunchInf
 }
 
 template <int N>
-bool launch_mixed_cw(const MixedArgs &A, int cw, int num_sms, cudaStream_t st, LaunchInfo *info) {
+void prepare_mixed_cw(int cw) {
+  if (cw == 4) mixed_attr<N, 4>();
+  if (cw == 8) mixed_attr<N, 8>();
+  if (cw == 11) mixed_attr<N, 11>();
+}
+
+template <int N>
+bool launch_mixed_cw(const MixedArgs &A, int cw, int ring_max, int num_sms, cudaStream_t st, LaunchInfo *info) {
   switch (cw) {
-    case 4: return launch_mixed_n<N, 4>(A, num_sms, st, info);
-    case 8: return launch_mixed_n<N, 8>(A, num_sms, st, info);
-    case 11: return launch_mixed_n<N, 11>(A, num_sms, st, info);
+    case 4: return launch_mixed_n<N, 4>(A, ring_max, num_sms, st, info);
+    case 8: return launch_mixed_n<N, 8>(A, ring_max, num_sms, st, info);
+    case 11: return launch_mixed_n<N, 11>(A, ring_max, num_sms, st, info);
     default: return false;
   }
 }
@@ -432,15 +466,26 @@ __global__ void split_join_kernel(SplitJoinArgs a) {
 
 }  // namespace
 
-bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st,
+bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int ring_max, int num_sms, cudaStream_t st,
                       LaunchInfo *info) {
   switch (N) {
-    case 1: return launch_mixed_cw<1>(A, consumer_warps, num_sms, st, info);
-    case 2: return launch_mixed_cw<2>(A, consumer_warps, num_sms, st, info);
-    case 3: return launch_mixed_cw<3>(A, consumer_warps, num_sms, st, info);
-    case 4: return launch_mixed_cw<4>(A, consumer_warps, num_sms, st, info);
-    case 5: return launch_mixed_cw<5>(A, consumer_warps, num_sms, st, info);
+    case 1: return launch_mixed_cw<1>(A, consumer_warps, ring_max, num_sms, st, info);
+    case 2: return launch_mixed_cw<2>(A, consumer_warps, ring_max, num_sms, st, info);
+    case 3: return launch_mixed_cw<3>(A, consumer_warps, ring_max, num_sms, st, info);
+    case 4: return launch_mixed_cw<4>(A, consumer_warps, ring_max, num_sms, st, info);
+    case 5: return launch_mixed_cw<5>(A, consumer_warps, ring_max, num_sms, st, info);
     default: return false;
+  }
+}
+
+void prepare_rhs_mixed(int N, int consumer_warps) {
+  switch (N) {
+    case 1: prepare_mixed_cw<1>(consumer_warps); break;
+    case 2: prepare_mixed_cw<2>(consumer_warps); break;
+    case 3: prepare_mixed_cw<3>(consumer_warps); break;
+    case 4: prepare_mixed_cw<4>(consumer_warps); break;
+    case 5: prepare_mixed_cw<5>(consumer_warps); break;
+    default: break;
   }
 }
 

@@ -370,7 +370,7 @@ struct MatmulOp : Op {
 // nz, Fscale (float64 or float32, read at build time only); gmap (int32, value indices into uhi's layout);
 // matrices Dr, Ds, Dt, LIFT, Fmask and Bary (Np x 4 barycentric coordinates of the nodes).
 struct MixedOp : Op {
-  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11;
+  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
   DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask;
   LaunchInfo info;
@@ -416,6 +416,8 @@ struct MixedOp : Op {
     conservative = R.flag("conservative", 0);
     warps = R.flag("warps", 11);
     require(warps == 4 || warps == 8 || warps == 11, R.kname + ": warps must be 4, 8 or 11");
+    ring = R.flag("ring", 0);
+    require(ring == 0 || (ring >= 2 && ring <= 24), R.kname + ": ring must be 0 (fill shared memory) or 2..24");
     uhi = R.array("uhi");
     ulo = R.array("ulo");
     uhin = R.array("uhiNext");
@@ -517,6 +519,7 @@ struct MixedOp : Op {
     tiles.upload(tl.data(), std::max<size_t>(tl.size(), 1) * sizeof(MTile));
   }
   std::vector<std::string> scalar_names() const override { return {"a", "b", "dt"}; }
+  void prepare(Runner &) override { prepare_rhs_mixed(N, warps); }
   void launch(Runner &r, const std::vector<double> &s) override {
     if (ntiles == 0) return;
     MixedArgs A{};
@@ -542,7 +545,7 @@ struct MixedOp : Op {
     A.dt = (float)s[2];
     A.conservative = conservative;
     A.status = r.status_word();
-    if (!launch_rhs_mixed(N, A, warps, r.num_sms, r.stream(), &info))
+    if (!launch_rhs_mixed(N, A, warps, ring, r.num_sms, r.stream(), &info))
       throw Error(DGK_ERR_UNSUPPORTED, "mixed stage: no launch shape fits shared memory for this order");
     std::swap(uhi->dptr, uhin->dptr);  // "uhi"/"ulo" always name the newest state
     std::swap(ulo->dptr, ulon->dptr);

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <sstream>
 
 namespace dgk {
@@ -495,22 +496,10 @@ void Runner::check_status(const char *what) {
   }
 }
 
-void Runner::execute_kernel(const char *kname, int nscalars, const double *scalars, void *const *host_ptrs) {
-  auto it = configs_.find(kname);
-  if (it == configs_.end())
-    throw Error(DGK_ERR_STATE, "kernel " + std::string(kname) + " not configured - use ConfigureKernel first");
-  KernelConfig &cfg = it->second;
-  need_device(__func__);
-  if (!cfg.op) throw Error(DGK_ERR_STATE, "kernel " + std::string(kname) + " not compiled - use BuildKernel first");
-  if (validate_) validate_offsets((std::string("before kernel ") + kname).c_str());
-  // pre-kernel copies (CopyTo)
-  for (size_t i = 0; i < cfg.params.size(); ++i)
-    if ((cfg.params[i].actions & DGK_COPY_TO) && host_ptrs && host_ptrs[i]) {
-      Binding &b = *cfg.params[i].b;
-      if (b.is_scalar) continue;
-      copy_to_device(b.name.c_str(), host_ptrs[i], b.total_values * dtype_size(b.host_dtype));
-    }
-  // scalar resolution (runner/kernel_execution.go:114-138)
+// Scalar resolution (runner/kernel_execution.go:114-138): bound scalars win over explicit values (with the
+// reference's warning), explicit values are taken in configuration order, and the result is ordered as the
+// operator consumes them.
+static std::vector<double> resolve_scalars(KernelConfig &cfg, int nscalars, const double *scalars) {
   std::map<std::string, double> sv;
   int sidx = 0;
   for (auto &pu : cfg.params) {
@@ -531,6 +520,25 @@ void Runner::execute_kernel(const char *kname, int nscalars, const double *scala
     if (f == sv.end()) throw Error(DGK_ERR_INVALID, "scalar " + s + " not provided");
     vals.push_back(f->second);
   }
+  return vals;
+}
+
+void Runner::execute_kernel(const char *kname, int nscalars, const double *scalars, void *const *host_ptrs) {
+  auto it = configs_.find(kname);
+  if (it == configs_.end())
+    throw Error(DGK_ERR_STATE, "kernel " + std::string(kname) + " not configured - use ConfigureKernel first");
+  KernelConfig &cfg = it->second;
+  need_device(__func__);
+  if (!cfg.op) throw Error(DGK_ERR_STATE, "kernel " + std::string(kname) + " not compiled - use BuildKernel first");
+  if (validate_) validate_offsets((std::string("before kernel ") + kname).c_str());
+  // pre-kernel copies (CopyTo)
+  for (size_t i = 0; i < cfg.params.size(); ++i)
+    if ((cfg.params[i].actions & DGK_COPY_TO) && host_ptrs && host_ptrs[i]) {
+      Binding &b = *cfg.params[i].b;
+      if (b.is_scalar) continue;
+      copy_to_device(b.name.c_str(), host_ptrs[i], b.total_values * dtype_size(b.host_dtype));
+    }
+  std::vector<double> vals = resolve_scalars(cfg, nscalars, scalars);
   cfg.op->launch(*this, vals);
   cuda_check(cudaGetLastError(), "kernel launch");
   if (validate_) validate_offsets((std::string("after kernel ") + kname).c_str());
@@ -543,6 +551,52 @@ void Runner::execute_kernel(const char *kname, int nscalars, const double *scala
       back = true;
     }
   if (back) check_status(kname);
+}
+
+Runner::Graph::~Graph() {
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+}
+
+// Capture nlaunch launches of one built kernel, launch l with scalars[l*nscalars ...], into one CUDA graph.
+// Operators that alternate ping-pong buffers swap them once per launch, so the count must be even for the
+// buffers named by the bindings to hold the newest state after every replay.  The launches are recorded, not
+// run: the state advances only when the graph is launched.
+Runner::Graph *Runner::capture_graph(const char *kname, int nlaunch, int nscalars, const double *scalars) {
+  need_device(__func__);
+  KernelConfig &cfg = config(kname);
+  if (!cfg.op) throw Error(DGK_ERR_STATE, "kernel " + std::string(kname) + " not compiled - use BuildKernel first");
+  if (nlaunch < 2 || nlaunch % 2)
+    throw Error(DGK_ERR_INVALID, "a captured sequence holds an even number (>= 2) of launches");
+  if (nscalars < 0 || (nscalars > 0 && !scalars)) throw Error(DGK_ERR_INVALID, "scalar rows missing");
+  for (auto &pu : cfg.params)
+    if (!pu.b->is_scalar && (pu.actions & (DGK_COPY_TO | DGK_COPY_BACK)))
+      throw Error(DGK_ERR_INVALID, "kernel " + std::string(kname) + ": a captured kernel carries no host copies");
+  std::vector<std::vector<double>> rows;
+  for (int l = 0; l < nlaunch; ++l) rows.push_back(resolve_scalars(cfg, nscalars, scalars + (size_t)l * nscalars));
+  cfg.op->prepare(*this);
+  cuda_check(cudaStreamSynchronize(stream_), "sync before capture");
+  std::unique_ptr<Graph> g(new Graph);
+  g->runner = this;
+  g->nlaunch = nlaunch;
+  cuda_check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+  try {
+    for (int l = 0; l < nlaunch; ++l) cfg.op->launch(*this, rows[(size_t)l]);
+  } catch (...) {
+    cudaGraph_t tmp = nullptr;
+    cudaStreamEndCapture(stream_, &tmp);
+    if (tmp) cudaGraphDestroy(tmp);
+    throw;
+  }
+  cuda_check(cudaStreamEndCapture(stream_, &g->graph), "cudaStreamEndCapture");
+  cuda_check(cudaGraphInstantiate(&g->exec, g->graph, 0), "cudaGraphInstantiate");
+  return g.release();
+}
+
+void Runner::launch_graph(Graph &g, int repeats) {
+  need_device(__func__);
+  if (g.runner != this) throw Error(DGK_ERR_INVALID, "graph belongs to another runner");
+  for (int i = 0; i < repeats; ++i) cuda_check(cudaGraphLaunch(g.exec, stream_), "cudaGraphLaunch");
 }
 
 void Runner::sync() {

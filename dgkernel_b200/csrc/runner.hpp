@@ -63,6 +63,8 @@ class Runner;
 struct Op {
   virtual ~Op() = default;
   virtual void launch(Runner &r, const std::vector<double> &scalars) = 0;
+  // Work that must happen before a stream capture records launches (function attributes and the like).
+  virtual void prepare(Runner &) {}
   // Scalar names the operator consumes, in the order it expects them.
   virtual std::vector<std::string> scalar_names() const { return {}; }
 };
@@ -105,6 +107,16 @@ class Runner {
   Binding *find(const std::string &name);
   KernelConfig &config(const std::string &name);
   void sync();
+  // A captured sequence of launches of one built kernel (stream capture -> CUDA graph), replayed as a unit.
+  struct Graph {
+    Runner *runner = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int nlaunch = 0;
+    ~Graph();
+  };
+  Graph *capture_graph(const char *kname, int nlaunch, int nscalars, const double *scalars);
+  void launch_graph(Graph &g, int repeats);
   void set_stream(cudaStream_t s) { stream_ = s ? s : own_stream_; }
   cudaStream_t stream() const { return stream_; }
   int *status_word() { return dstatus_; }

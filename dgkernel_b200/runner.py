@@ -436,6 +436,38 @@ class Runner:
         for n in later:
             self._copy(n, False)
 
+    def CaptureGraph(self, name: str, scalar_rows) -> Graph:
+        """Record len(scalar_rows) (even) launches of kernel `name`, row l giving launch l's scalars, into one
+        CUDA graph.  Nothing runs until Graph.Launch; ping-pong operators leave the bindings naming the newest
+        state after every replay."""
+        rows = np.ascontiguousarray(np.asarray(scalar_rows, dtype=np.float64).reshape(len(scalar_rows), -1))
+        h = C.c_void_p()
+        self._check(lib().dgk_capture_graph(self._h, name.encode(), rows.shape[0], rows.shape[1],
+                                            rows.ctypes.data_as(C.POINTER(C.c_double)), C.byref(h)))
+        return Graph(self, h, rows.shape[0])
+
+
+class Graph:
+    """A captured sequence of launches of one built kernel (CUDA graph); Launch replays it on the runner's
+    stream.  Free it before its runner."""
+
+    def __init__(self, runner: "Runner", handle, nlaunch: int):
+        self.runner, self._h, self.nlaunch = runner, handle, nlaunch
+
+    def Launch(self, repeats: int = 1):
+        self.runner._check(lib().dgk_graph_launch(self._h, int(repeats)))
+
+    def Free(self):
+        if getattr(self, "_h", None):
+            lib().dgk_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.Free()
+        except Exception:
+            pass
+
 
 def NewRunner(config: Config, **kw) -> Runner:
     return Runner(config, **kw)

@@ -57,6 +57,7 @@ extern "C" {
 
 typedef struct dgk_runner dgk_runner;
 typedef struct dgk_element dgk_element;
+typedef struct dgk_graph dgk_graph;
 
 /* ---- runner lifecycle --------------------------------------------------------------------------- */
 /* NewRunner + builder.NewBuilder (runner/runner.go:48-86, runner/builder/builder.go:73-100).
@@ -74,6 +75,20 @@ const char *dgk_global_error(void);
 int dgk_set_stream(dgk_runner *r, void *cuda_stream);
 /* Device.Finish (runner/kernel_execution.go:62). */
 int dgk_sync(dgk_runner *r);
+
+/* ---- captured launch sequences ------------------------------------------------------------------- */
+/* No counterpart in the reference, whose ExecuteKernel (runner/kernel_execution.go:12-89) runs one kernel
+ * per call.  Record nlaunch (even, >= 2) consecutive launches of a built kernel, launch l taking the
+ * nscalars values at scalars + l*nscalars, into one CUDA graph on the runner's stream; nothing runs until
+ * dgk_graph_launch.  Operators that alternate ping-pong buffers swap them once per recorded launch, so
+ * after every replay the bindings name the newest state.  The kernel's configuration may carry no host
+ * copies.  A graph is tied to its runner: free it before the runner. */
+int dgk_capture_graph(dgk_runner *r, const char *kernel_name, int32_t nlaunch, int32_t nscalars,
+                      const double *scalars, dgk_graph **out);
+/* Launch a captured sequence `repeats` times on the runner's stream (asynchronous; dgk_sync reports the
+ * kernels' status word). */
+int dgk_graph_launch(dgk_graph *g, int32_t repeats);
+int dgk_graph_free(dgk_graph *g);
 
 /* ---- bindings (DefineBindings, runner/binding.go:100-195) --------------------------------------- */
 /* Array or temp binding.  part_values (part_count entries) gives the host values of each partition of a
@@ -192,6 +207,10 @@ int dgk_setup_geometry(dgk_runner *r, const dgk_element *e, int64_t nverts, cons
  * kind 2: mean + sum_m a_m cos(pi (k_m . x) + phi_m) with modes rows (kx, ky, kz, a, phi). */
 int dgk_init_field(dgk_runner *r, const char *name, const char *xname, const char *yname, const char *zname,
                    int32_t kind, double mean, double amp, int32_t nmodes, const double *modes);
+/* As dgk_init_field with kind 2, but every partition (for example every independent instance of a batch)
+ * takes its own nmodes modes: modes holds npart * nmodes rows, partition p's rows first at p * nmodes. */
+int dgk_init_field_parts(dgk_runner *r, const char *name, const char *xname, const char *yname, const char *zname,
+                         double mean, int32_t nmodes, const double *modes);
 /* splitmix64 uniform stream (53-bit doubles), for reproducible inputs across host and oracle. */
 int dgk_splitmix_uniform(uint64_t seed, int64_t count, double *out);
 
