@@ -49,6 +49,10 @@ SIGNATURES = {
     "dgk_face_connector": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI64, _PI64],
     "dgk_face_gather_map": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI32],
     "dgk_init_field_parts": [_P, _S, _S, _S, _S, _D, _I32, _PD],
+    "dgk_mlp_param_count": [_I32, _PI64],
+    "dgk_mlp_forward": [_P, _P, _I64, _I32, _I32, _P, _P, _P],
+    "dgk_mlp_loss_grad": [_P, _P, _P, _I64, _I32, _P, _P, _P],
+    "dgk_mlp_adam": [_P, _P, _P, _P, _I64, C.c_float, C.c_float, C.c_float, C.c_float, _I32, _P],
     "dgk_capture_graph": [_P, _S, _I32, _I32, _PD, C.POINTER(_P)],
     "dgk_graph_launch": [_P, _I32],
     "dgk_graph_free": [_P],

@@ -16,6 +16,12 @@ from .element import Element
 from .runner import (Config, Float32, Float64, INT32, INT64, Runner, Scalar, Temp, Input, WarpAlign)
 from ._lib import check, lib
 
+
+def mlp_param_count(nin: int) -> int:
+    n = C.c_int64()
+    check(lib().dgk_mlp_param_count(int(nin), C.byref(n)))
+    return n.value
+
 import ctypes as C
 
 # Carpenter-Kennedy five-stage LSERK4 (examples/3d_scalar_burgers_equation.go:138-151)
@@ -110,8 +116,9 @@ class _TetBurgers:
     dtype "mixed": the mixed-precision stage (`rhsStageMixed`): compensated FP32 state uhi + ulo, FP32
     residual, compact affine geometry derived from the FP64 metrics; `get("u")` joins the pair in FP64."""
 
-    def _assemble(self, N, VX, VY, VZ, EToV, EToE, EToF, EToP, Kpart, dtype, stream):
+    def _assemble(self, N, VX, VY, VZ, EToV, EToE, EToF, EToP, Kpart, dtype, stream, viscosity=None):
         self.N = N
+        self.visc = viscosity
         self.mixed = isinstance(dtype, str) and dtype == MIXED
         self.dtype = np.dtype(np.float64) if self.mixed else np.dtype(dtype)
         dt_code = Float64 if self.dtype == np.float64 else Float32
@@ -132,6 +139,14 @@ class _TetBurgers:
             params += [Temp(nm).Type(Float32).Size(K * Np).Align(WarpAlign)
                        for nm in ("uhi", "ulo", "uhiNext", "uloNext", "resu")]
             params += [Input(f"Bary_{sn}").Bind(bary_matrix(el)).ToMatrix().Static()]
+        if self.visc:
+            if self.mixed or self.dtype != np.float64:
+                raise ValueError("the artificial-viscosity stage runs in float64")
+            params += [Temp(nm).Type(Float64).Size(K * Np) for nm in ("eps", "qx", "qy", "qz")]
+            params += [Temp("feat").Type(Float32).Size(K * Np), Temp("sigma").Type(Float32).Size(K),
+                       Temp("mlpSigma").Type(Float32).Size(K)]
+            params += [Input(f"Vinv_{sn}").Bind(el.Vinv).ToMatrix().Static()]
+            params += [Input("MLP").Bind(np.zeros((1, mlp_param_count(Np)))).ToMatrix().DeviceMemType(Float32)]
         params += [Input(f"{m}_{sn}").Bind(getattr(el, m)).ToMatrix().Static() for m in ("Dr", "Ds", "Dt", "LIFT")]
         params += [Input("Fmask").Bind(el.Fmask.astype(np.float64)).ToMatrix().DeviceMemType(INT32)]
         params += [Scalar("a").Type(Float64), Scalar("b").Type(Float64), Scalar("dt").Type(Float64)]
@@ -151,7 +166,7 @@ class _TetBurgers:
         self.gmap = M.face_gather_map(K, 4, Nfp, Np, self.vmapP, EToP, self.node_off)
         r.CopyToDevice("gmap", self.gmap)
 
-    def _finish(self, cfl, conservative, warps=None, ring=None):
+    def _finish(self, cfl, conservative, warps=None, ring=None, eps0=1.0, c0=0.0, kappa=1.0, conf=(0.1, 0.9)):
         r, el = self.runner, self.el
         sn = el.ShortName
         fixed_m = [f"Dr_{sn}", f"Ds_{sn}", f"Dt_{sn}", f"LIFT_{sn}", "Fmask"]
@@ -167,12 +182,29 @@ class _TetBurgers:
         self.conservative = conservative
         self.u0 = self.get("u")
         self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))
+        if self.visc:
+            self.av = {"eps0": eps0, "c0": c0, "kappa": kappa, "lo": conf[0], "hi": conf[1]}
+            fs = self.get("Fscale").reshape(self.K, -1)
+            self.eps_max = eps0 * float(np.max(2.0 / fs.max(axis=1))) / self.N
+            if self.eps_max > 0:  # diffusive limit of the explicit step
+                self.dt = min(self.dt, cfl * self.hmin ** 2 / self.eps_max)
+            sn = self.el.ShortName
+            fixed += ["eps", "qx", "qy", "qz", f"Vinv_{sn}", "MLP"]
+            feats = ["u", *GEO, *FACE, "gmap", *fixed_m, f"Vinv_{sn}", "MLP", "feat", "sigma", "mlpSigma"]
+            r.ConfigureKernel("sensorFeatures", *[r.Param(p) for p in feats])
         r.ConfigureKernel("rhsStage", *[r.Param(p) for p in fixed], r.Param("a"), r.Param("b"), r.Param("dt"))
         self.stage = 0
         self.build_stage(warps=warps, ring=ring)
 
+    def _av_args(self, sensor):
+        a = self.av
+        return (f"sensor={sensor},eps0={a['eps0']!r},c0={a['c0']!r},kappa={a['kappa']!r},"
+                f"lo={a['lo']!r},hi={a['hi']!r}")
+
     def op_id(self, warps=None, ring=None) -> str:
         """Operator id of the stage kernel, with the launch shape (mixed stage) when given."""
+        if self.visc:
+            return f"rhsStageAV({self._av_args(self.visc)})"
         if not self.mixed:
             return f"rhsStage(conservative={self.conservative})"
         args = [f"conservative={self.conservative}"]
@@ -186,6 +218,32 @@ class _TetBurgers:
         """(Re)build the stage operator, optionally with a given launch shape."""
         self.shape = {"warps": warps, "ring": ring}
         self.runner.BuildKernel(self.op_id(warps, ring), "rhsStage")
+
+    def set_sensor(self, sensor: str, params=None):
+        """Viscosity stage: switch the sensor ("none", "pp" or "mlp"; for "mlp" the network's float32
+        parameters) and rebuild the stage."""
+        if not self.visc:
+            raise ValueError("problem built without viscosity")
+        if params is not None:
+            self.runner.CopyToDevice("MLP", np.asarray(params, dtype=np.float64).reshape(1, -1))
+        self.visc = sensor
+        self.build_stage()
+
+    def sensor_features(self, sensor: str = "pp"):
+        """(unit-norm modal coefficients [K, Np], PP activation [K], network output [K] or None) of the current
+        state, from the stage's own sensor pass."""
+        r = self.runner
+        r.BuildKernel(f"sensorFeatures({self._av_args(sensor)})", "sensorFeatures")
+        r.ExecuteKernel("sensorFeatures")
+        feat = np.zeros(self.K * self.el.Np, dtype=np.float32)
+        sig = np.zeros(self.K, dtype=np.float32)
+        r.CopyFromDevice("feat", feat)
+        r.CopyFromDevice("sigma", sig)
+        mo = None
+        if sensor == "mlp":
+            mo = np.zeros(self.K, dtype=np.float32)
+            r.CopyFromDevice("mlpSigma", mo)
+        return feat.reshape(self.K, self.el.Np), sig, mo
 
     @property
     def dofs(self) -> int:
@@ -237,21 +295,23 @@ class BurgersProblem(_TetBurgers):
     partitions (u0: "sine", "shock", "smooth" or "modes"; dtype float64, float32 or "mixed")."""
 
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
-                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None):
+                 cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None,
+                 viscosity=None, eps0: float = 1.0, c0: float = 0.0, kappa: float = 1.0, conf=(0.1, 0.9),
+                 mode_sigma: float = 0.1):
         self.n, self.nslab = n, nslab
         VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)
         EToE, EToF = M.ti_connect3d(EToVp)
         K = EToV.shape[0]
-        self._assemble(N, VX, VY, VZ, EToV, EToE, EToF, EToP, [K // nslab] * nslab, dtype, stream)
+        self._assemble(N, VX, VY, VZ, EToV, EToE, EToF, EToP, [K // nslab] * nslab, dtype, stream, viscosity)
         r = self.runner
         if u0_host is not None:
             r.CopyToDevice("u", np.ascontiguousarray(u0_host, dtype=self.dtype).reshape(-1))
         else:
             kinds = {"sine": (0, 0.0, 0.5), "shock": (0, 0.5, 1.0), "smooth": (1, 0.5, 0.25), "modes": (2, 0.5, 0.0)}
             kind, mean, amp = kinds[u0]
-            modes = random_modes(seed) if kind == 2 else np.zeros((0, 5))
+            modes = random_modes(seed, sigma=mode_sigma) if kind == 2 else np.zeros((0, 5))
             check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, len(modes), _pd(modes)), r._h)
-        self._finish(cfl, conservative, warps, ring)
+        self._finish(cfl, conservative, warps, ring, eps0, c0, kappa, conf)
 
 
 class BurgersEnsemble(_TetBurgers):

@@ -390,6 +390,41 @@ int dgk_init_field_parts(dgk_runner *r, const char *name, const char *xn, const 
   return guard(r, [&] { init_field(r, name, xn, yn, zn, 2, mean, 0.0, nmodes, modes, true); });
 }
 
+int dgk_mlp_param_count(int32_t nin, int64_t *count) {
+  return guard(nullptr, [&] {
+    if (!count) throw dgk::Error(DGK_ERR_INVALID, "null output");
+    *count = dgk::mlp_param_count(nin);
+  });
+}
+
+int dgk_mlp_forward(const float *params, const float *X, int64_t n, int32_t nin, int32_t fp16, float *out,
+                    void *half_scratch, void *cuda_stream) {
+  return guard(nullptr, [&] {
+    if (n < 0 || (n > 0 && (!params || !X || !out)) || (fp16 && !half_scratch))
+      throw dgk::Error(DGK_ERR_INVALID, "mlp forward: null buffer or negative count");
+    if (n == 0) return;
+    dgk::launch_mlp_forward(params, X, n, nin, out, fp16, half_scratch, static_cast<cudaStream_t>(cuda_stream));
+  });
+}
+
+int dgk_mlp_loss_grad(const float *params, const float *X, const float *y, int64_t n, int32_t nin, float *grad,
+                      float *loss, void *cuda_stream) {
+  return guard(nullptr, [&] {
+    if (n <= 0 || !params || !X || !y || !grad || !loss)
+      throw dgk::Error(DGK_ERR_INVALID, "mlp gradient: null buffer or no samples");
+    dgk::launch_mlp_grad(params, X, y, n, nin, grad, loss, static_cast<cudaStream_t>(cuda_stream));
+  });
+}
+
+int dgk_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t count, float lr, float beta1,
+                 float beta2, float eps, int32_t step, void *cuda_stream) {
+  return guard(nullptr, [&] {
+    if (count <= 0 || !params || !grad || !m || !v || step < 1)
+      throw dgk::Error(DGK_ERR_INVALID, "adam: null buffer, empty parameter set or step < 1");
+    dgk::launch_adam(params, grad, m, v, count, lr, beta1, beta2, eps, step, static_cast<cudaStream_t>(cuda_stream));
+  });
+}
+
 int dgk_capture_graph(dgk_runner *r, const char *kernel_name, int32_t nlaunch, int32_t nscalars,
                       const double *scalars, dgk_graph **out) {
   return guard(r, [&] {

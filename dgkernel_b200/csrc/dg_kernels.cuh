@@ -145,4 +145,42 @@ struct SplitJoinArgs {
   float *hi, *lo;
 };
 
+// ---- artificial-viscosity stage and shock-sensor MLP (av.cu) ----
+struct AvTile {
+  int64_t node_base;  // value index of the tile's first element in node arrays
+  int64_t face_base;  // value index of the tile's first element in face arrays
+  int64_t elem_base;  // global index of the tile's first element (the operator's own per-element arrays)
+  int64_t e1_base;    // value index in bound per-element arrays (one value per element)
+  int64_t feat_base;  // value index in a bound feature array (Np values per element)
+  int32_t nelem, part;
+};
+
+struct AvArgs {
+  const AvTile *tiles;
+  int ntiles;
+  const double *u;      // state read by this stage (and the neighbour traces)
+  double *u_out;        // state written (ping-pong partner)
+  double *resu;         // LSERK residual, in place
+  double *q[3];         // BR1 gradient (x, y, z), node arrays
+  double *eps;          // viscosity per node (constant per element)
+  const double *geo[9];
+  const double *face[4];
+  const int32_t *gmap;
+  int64_t n_u_values;
+  const double *Dr, *Ds, *Dt, *Vinv;  // row-major Np x Np
+  const double *LIFT;                 // row-major Np x 4Nfp
+  const int32_t *fmask;               // [4 Nfp]
+  const int32_t *top;                 // [Np] 1 for the modes of total degree N
+  const double *h_over_n;             // per element: (2 / max Fscale) / N
+  int mode;                           // 0: no viscosity, 1: PP sensor, 2: MLP sensor with PP fallback
+  double eps0, s0, kappa;
+  float conf_lo, conf_hi;             // MLP outputs inside (lo, hi) fall back to the PP activation
+  const unsigned short *mlp16;        // MLP parameters as FP16 bits
+  float *S_out, *sig_out, *feat_out, *mlp_out;  // optional per-element sensor outputs
+  unsigned int *fallback_count;       // optional
+  double a, b, dt;
+  int prep_only;                      // 1: sensor / gradient pass only
+  int *status;
+};
+
 }  // namespace dgk

@@ -37,6 +37,18 @@ template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);
 void launch_split_join(const SplitJoinArgs &a, cudaStream_t st);
 
+// Artificial-viscosity stage and the sensor MLP (av.cu).
+void launch_av(int N, const AvArgs &A, int num_sms, cudaStream_t st);
+int mlp_param_count(int nin);
+int av_tile_elems(int N);  // elements per tile of the viscosity kernels
+void launch_to_half(const float *in, void *out, int64_t n, cudaStream_t st);
+void launch_mlp_forward(const float *p, const float *X, int64_t n, int nin, float *out, int fp16, void *half_buf,
+                        cudaStream_t st);
+void launch_mlp_grad(const float *p, const float *X, const float *y, int64_t n, int nin, float *grad, float *loss,
+                     cudaStream_t st);
+void launch_adam(float *p, const float *g, float *m, float *v, int64_t P, float lr, float b1, float b2, float eps,
+                 int step, cudaStream_t st);
+
 // Generic MATMUL_<M> over partitions: out[e*rows + i] (+)= sum_j M[i][j] in[e*cols + j].
 template <typename T>
 void launch_matmul(const T *M_rowmajor, int rows, int cols, const T *in, T *out, const int64_t *d_in_off,

@@ -80,6 +80,14 @@ struct Roles {
     auto it = explicit_.find(k);
     return it == explicit_.end() ? dflt : std::atoi(it->second.c_str());
   }
+  double num(const std::string &k, double dflt) {
+    auto it = explicit_.find(k);
+    return it == explicit_.end() ? dflt : std::atof(it->second.c_str());
+  }
+  std::string word(const std::string &k, const std::string &dflt) {
+    auto it = explicit_.find(k);
+    return it == explicit_.end() ? dflt : it->second;
+  }
 };
 
 int order_from_np(int64_t np) {
@@ -99,9 +107,13 @@ struct DevBuf {
     return static_cast<T *>(p);
   }
   void upload(const void *h, size_t bytes) {
-    if (p) cudaFree(p);
-    cuda_check(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc(op buffer)");
+    alloc(bytes);
     cuda_check(cudaMemcpy(p, h, bytes, cudaMemcpyHostToDevice), "upload op buffer");
+  }
+  void alloc(size_t bytes) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cuda_check(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc(op buffer)");
   }
 };
 
@@ -587,6 +599,182 @@ struct SplitJoinOp : Op {
   }
 };
 
+
+// Artificial-viscosity stage (av.cu): the plain FP64 stage plus BR1 viscosity eps_e = eps0 sigma_e h_e / N
+// from a modal shock sensor.  Op id: rhsStageAV(sensor=none|pp|mlp, eps0=1, c0=0, kappa=1, lo=0.1, hi=0.9);
+// the PP switch point is s0 = -(c0 + 4 log10 N).  Roles: u, uNext, resu, Rx..Tz, nx, ny, nz, Fscale, gmap,
+// eps, qx, qy, qz (float64 node arrays), matrices Dr, Ds, Dt, LIFT, Fmask, Vinv and, for sensor=mlp, MLP (1 x P
+// float32 parameters, read from the device at every launch).  sensorFeatures: the sensor pass alone, writing
+// feat (float32, Np per element: unit-norm modal coefficients), sigma (float32 per element: PP activation)
+// and, with an MLP role, mlpSigma (the network's output).
+struct AvOp : Op {
+  int N = 0, mode = 1, ntiles = 0, features = 0;
+  int64_t np = 0;
+  double eps0 = 1.0, s0 = 0.0, kappa = 1.0;
+  float lo = 0.1f, hi = 0.9f;
+  Binding *u, *unext = nullptr, *resu = nullptr, *geo[9], *face[4], *gmap, *eps = nullptr, *q[3] = {};
+  Binding *mlp = nullptr, *feat = nullptr, *sig = nullptr, *mlps = nullptr;
+  DevBuf tiles, dr, ds, dt, vinv, lift, fmask, top, hon, mlp16, qs[3], epsb;
+  AvOp(Runner &r, Roles &R, int feats) : features(feats) {
+    static const char *gn[9] = {"Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz"};
+    static const char *fn[4] = {"nx", "ny", "nz", "Fscale"};
+    const std::string sensor = lower(R.word("sensor", "pp"));
+    if (sensor == "none") mode = 0;
+    else if (sensor == "pp") mode = 1;
+    else if (sensor == "mlp") mode = 2;
+    else throw Error(DGK_ERR_INVALID, R.kname + ": sensor must be none, pp or mlp");
+    eps0 = R.num("eps0", 1.0);
+    kappa = R.num("kappa", 1.0);
+    lo = (float)R.num("lo", 0.1);
+    hi = (float)R.num("hi", 0.9);
+    require(kappa > 0.0 && eps0 >= 0.0, R.kname + ": kappa > 0 and eps0 >= 0");
+    u = R.array("u");
+    require(u->dev_dtype == DGK_FLOAT64, R.kname + ": the viscosity stage runs in float64");
+    for (int i = 0; i < 9; ++i) geo[i] = R.array(gn[i]);
+    for (int i = 0; i < 4; ++i) face[i] = R.array(fn[i]);
+    gmap = R.array("gmap");
+    Binding *Dr = R.matrix("Dr"), *Ds = R.matrix("Ds"), *Dt = R.matrix("Dt"), *L = R.matrix("LIFT"),
+            *fm = R.matrix("Fmask"), *Vi = R.matrix("Vinv");
+    np = Dr->rows;
+    N = order_from_np(np);
+    require(N <= 5, R.kname + ": orders 1..5");
+    s0 = -(R.num("c0", 0.0) + 4.0 * std::log10((double)N));
+    const int nfp = (N + 1) * (N + 2) / 2, nf = 4 * nfp;
+    require(u->values_per_elem == np, R.kname + ": u must hold Np values per element");
+    for (Binding *b : geo) same_layout(*u, *b, R.kname);
+    require(face[0]->values_per_elem == nf && face[0]->dev_dtype == DGK_FLOAT64,
+            R.kname + ": face arrays must be float64 with 4*Nfp values per element");
+    for (Binding *b : face) same_layout(*face[0], *b, R.kname);
+    require(gmap->dev_dtype == DGK_INT32 && gmap->values_per_elem == nf && gmap->offsets == face[0]->offsets,
+            R.kname + ": gmap must be int32 with the face arrays' layout");
+    require(L->rows == np && L->cols == nf && Vi->rows == np && Vi->cols == np, R.kname + ": LIFT / Vinv shapes");
+    if (mode == 2) {
+      mlp = R.matrix("MLP");
+      require(mlp->rows * mlp->cols == mlp_param_count((int)np) && mlp->dev_dtype == DGK_FLOAT32,
+              R.kname + ": MLP must hold " + std::to_string(mlp_param_count((int)np)) + " float32 parameters");
+      std::vector<uint16_t> z((size_t)mlp_param_count((int)np) + 8, 0);
+      mlp16.upload(z.data(), z.size() * sizeof(uint16_t));
+    }
+    if (features) {
+      feat = R.array("feat");
+      sig = R.array("sigma");
+      mlps = R.array("mlpSigma", false);
+      require(feat->dev_dtype == DGK_FLOAT32 && feat->values_per_elem == np, R.kname + ": feat is float32, Np per element");
+      require(sig->dev_dtype == DGK_FLOAT32 && sig->values_per_elem == 1, R.kname + ": sigma is float32, 1 per element");
+      if (mlps) same_layout(*sig, *mlps, R.kname);
+      // the gradient and viscosity outputs of the sensor pass go to operator-owned scratch
+      const size_t nb = sizeof(double) * (size_t)u->offsets.back();
+      for (auto &b : qs) b.alloc(nb);
+      epsb.alloc(nb);
+    } else {
+      unext = R.array("uNext");
+      resu = R.array("resu");
+      eps = R.array("eps");
+      q[0] = R.array("qx");
+      q[1] = R.array("qy");
+      q[2] = R.array("qz");
+      for (Binding *b : {unext, resu, eps, q[0], q[1], q[2]}) same_layout(*u, *b, R.kname);
+    }
+    auto rm = [&](Binding *m, DevBuf &d) { d.upload(m->mat.data(), m->mat.size() * sizeof(double)); };
+    rm(Dr, dr);
+    rm(Ds, ds);
+    rm(Dt, dt);
+    rm(Vi, vinv);
+    rm(L, lift);
+    std::vector<int32_t> fmi(fm->mat.begin(), fm->mat.end());
+    for (int32_t v : fmi) require(v >= 0 && v < np, R.kname + ": Fmask entry out of range");
+    fmask.upload(fmi.data(), fmi.size() * sizeof(int32_t));
+    std::vector<int32_t> tp;
+    for (int i = 0; i <= N; ++i)  // modes ordered i, j, k (vandermonde3d.go:15-42)
+      for (int j = 0; j <= N - i; ++j)
+        for (int k = 0; k <= N - i - j; ++k) tp.push_back(i + j + k == N ? 1 : 0);
+    top.upload(tp.data(), tp.size() * sizeof(int32_t));
+    // h_e / N with h_e = 2 / max Fscale over the element's face points
+    std::vector<double> fs((size_t)face[3]->offsets.back());
+    cuda_check(cudaMemcpy(fs.data(), face[3]->dptr, fs.size() * sizeof(double), cudaMemcpyDeviceToHost), "Fscale");
+    std::vector<double> h;
+    std::vector<AvTile> tl;
+    const int te = av_tile_elems(N);
+    int64_t eg = 0;
+    for (int p = 0; p < r.npart; ++p) {
+      for (int64_t e = 0; e < r.K[p]; ++e) {
+        double m = 0.0;
+        for (int k = 0; k < nf; ++k) m = std::max(m, fs[(size_t)(face[3]->offsets[p] + e * nf + k)]);
+        require(m > 0.0, R.kname + ": Fscale must be positive");
+        h.push_back(2.0 / m / N);
+      }
+      for (int64_t s0e = 0; s0e < r.K[p]; s0e += te) {
+        AvTile x{};
+        x.node_base = u->offsets[p] + s0e * np;
+        x.face_base = face[0]->offsets[p] + s0e * nf;
+        x.elem_base = eg + s0e;
+        x.e1_base = sig ? sig->offsets[p] + s0e : 0;
+        x.feat_base = feat ? feat->offsets[p] + s0e * np : 0;
+        x.nelem = (int32_t)std::min<int64_t>(te, r.K[p] - s0e);
+        x.part = p;
+        tl.push_back(x);
+      }
+      eg += r.K[p];
+    }
+    hon.upload(h.data(), std::max<size_t>(h.size(), 1) * sizeof(double));
+    ntiles = (int)tl.size();
+    tiles.upload(tl.data(), std::max<size_t>(tl.size(), 1) * sizeof(AvTile));
+  }
+  std::vector<std::string> scalar_names() const override {
+    if (features) return {};
+    return {"a", "b", "dt"};
+  }
+  void launch(Runner &r, const std::vector<double> &s) override {
+    if (ntiles == 0) return;
+    AvArgs A{};
+    A.tiles = tiles.get<AvTile>();
+    A.ntiles = ntiles;
+    A.u = reinterpret_cast<const double *>(u->dptr);
+    for (int i = 0; i < 9; ++i) A.geo[i] = reinterpret_cast<const double *>(geo[i]->dptr);
+    for (int i = 0; i < 4; ++i) A.face[i] = reinterpret_cast<const double *>(face[i]->dptr);
+    A.gmap = reinterpret_cast<const int32_t *>(gmap->dptr);
+    A.n_u_values = u->offsets.back();
+    A.Dr = dr.get<double>();
+    A.Ds = ds.get<double>();
+    A.Dt = dt.get<double>();
+    A.Vinv = vinv.get<double>();
+    A.LIFT = lift.get<double>();
+    A.fmask = fmask.get<int32_t>();
+    A.top = top.get<int32_t>();
+    A.h_over_n = hon.get<double>();
+    A.mode = mode;
+    A.eps0 = eps0;
+    A.s0 = s0;
+    A.kappa = kappa;
+    A.conf_lo = lo;
+    A.conf_hi = hi;
+    A.status = r.status_word();
+    if (mode == 2) {
+      launch_to_half(reinterpret_cast<const float *>(mlp->dptr), mlp16.p, mlp_param_count((int)np), r.stream());
+      A.mlp16 = mlp16.get<unsigned short>();
+    }
+    if (features) {
+      for (int d = 0; d < 3; ++d) A.q[d] = qs[d].get<double>();
+      A.eps = epsb.get<double>();
+      A.feat_out = reinterpret_cast<float *>(feat->dptr);
+      A.sig_out = reinterpret_cast<float *>(sig->dptr);
+      A.mlp_out = mlps ? reinterpret_cast<float *>(mlps->dptr) : nullptr;
+      A.prep_only = 1;
+      launch_av(N, A, r.num_sms, r.stream());
+      return;
+    }
+    A.u_out = reinterpret_cast<double *>(unext->dptr);
+    A.resu = reinterpret_cast<double *>(resu->dptr);
+    for (int d = 0; d < 3; ++d) A.q[d] = reinterpret_cast<double *>(q[d]->dptr);
+    A.eps = reinterpret_cast<double *>(eps->dptr);
+    A.a = s[0];
+    A.b = s[1];
+    A.dt = s[2];
+    launch_av(N, A, r.num_sms, r.stream());
+    std::swap(u->dptr, unext->dptr);
+  }
+};
+
 template <template <typename> class O, typename... A>
 std::unique_ptr<Op> typed(int dt, Runner &r, Roles &R, A... a) {
   if (dt == DGK_FLOAT64) return std::make_unique<O<double>>(r, R, a...);
@@ -608,6 +796,8 @@ std::unique_ptr<Op> make_op(Runner &r, KernelConfig &cfg, const std::string &op_
   if (name == "rhsStage") return typed<RhsOp>(R.array("u")->dev_dtype, r, R, 0);
   if (name == "rhsLF") return typed<RhsOp>(R.array("u")->dev_dtype, r, R, 1);
   if (name == "rhsStageMixed") return std::make_unique<MixedOp>(r, R);
+  if (name == "rhsStageAV") return std::make_unique<AvOp>(r, R, 0);
+  if (name == "sensorFeatures") return std::make_unique<AvOp>(r, R, 1);
   if (name == "splitState") return std::make_unique<SplitJoinOp>(r, R, 0);
   if (name == "joinState") return std::make_unique<SplitJoinOp>(r, R, 1);
   if (name == "matmul") return typed<MatmulOp>(R.array("IN")->dev_dtype, r, R, 0);

@@ -214,6 +214,23 @@ int dgk_init_field_parts(dgk_runner *r, const char *name, const char *xname, con
 /* splitmix64 uniform stream (53-bit doubles), for reproducible inputs across host and oracle. */
 int dgk_splitmix_uniform(uint64_t seed, int64_t count, double *out);
 
+/* ---- shock-sensor network (learned sensor of the artificial-viscosity stage) ---------------------------
+ * No counterpart in the reference, which has no sensor.  A 3-layer perceptron nin -> 32 -> 32 -> 1 (tanh,
+ * tanh, sigmoid); parameters are `count` float32 values W1[32][nin], b1[32], W2[32][32], b2[32], w3[32], b3,
+ * with nin = Np of orders 1..5.  All arrays are device pointers; work is queued on cuda_stream (NULL: the
+ * default stream) and the calls return without synchronising. */
+int dgk_mlp_param_count(int32_t nin, int64_t *count);
+/* out[s] = network(X[s, :]) for n samples; fp16 = 1 rounds the weights to FP16 first (sums stay FP32, the
+ * arithmetic of the stage's sensor), which needs `half_scratch` of count 2-byte values. */
+int dgk_mlp_forward(const float *params, const float *X, int64_t n, int32_t nin, int32_t fp16, float *out,
+                    void *half_scratch, void *cuda_stream);
+/* grad = d/dparams of mean_s (network(X[s]) - y[s])^2 and loss = that mean (both overwritten). */
+int dgk_mlp_loss_grad(const float *params, const float *X, const float *y, int64_t n, int32_t nin, float *grad,
+                      float *loss, void *cuda_stream);
+/* One Adam step (bias-corrected, step counted from 1) on `count` parameters with moments m and v. */
+int dgk_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t count, float lr, float beta1,
+                 float beta2, float eps, int32_t step, void *cuda_stream);
+
 /* ---- allocation-free upload ----------------------------------------------------------------------- */
 /* No counterpart in the reference.  Converting upload that allocates nothing: `count` host values of
  * host_dtype are staged in a fixed 8 MiB array inside the library's device image and converted on the GPU

@@ -286,3 +286,195 @@ int ora_max_threads(void)
     return 1;
 #endif
 }
+
+/* ---- artificial viscosity with a modal shock sensor (the build's fixed formulas; parity unpinned) ----
+ *
+ * Sensor (Persson & Peraire): uhat = Vinv u per element (orthonormal modes, element/library/gonudg/
+ * simplex3dp.go:15-36, order i, j, k of vandermonde3d.go:15-42); S = log10(sum over modes of total degree N
+ * of uhat^2 / sum over all modes of uhat^2); activation sigma = 0 for S < s0 - kappa, 1 for S > s0 + kappa,
+ * else (1 + sin(pi (S - s0) / (2 kappa))) / 2.  Viscosity eps_e = eps0 sigma_e h_e / N with h_e = 2 / max
+ * of the element's Fscale.  Learned mode: sigma = MLP(uhat / |uhat|) (nin -> 32 -> 32 -> 1, tanh, tanh,
+ * sigmoid) where the MLP output lies outside (conf_lo, conf_hi), the PP sigma inside that band.
+ *
+ * Viscous term (BR1, central fluxes): q_d = D_d u + LIFT (Fscale n_d (uP - uM) / 2), d = x, y, z; then
+ * rhs += eps_e sum_d D_d q_d + LIFT (Fscale 1/2 sum_d n_d (epsP qP_d - epsM qM_d)). */
+
+static double pp_sigma(double S, double s0, double kappa)
+{
+    if (!(S >= s0 - kappa)) return 0.0; /* also S = -inf (an element with no energy) */
+    if (S > s0 + kappa) return 1.0;
+    return 0.5 * (1.0 + sin(M_PI * (S - s0) / (2.0 * kappa)));
+}
+
+double ora_mlp_forward1(int nin, const double *p, const double *x)
+{
+    const double *W1 = p, *b1 = W1 + 32 * nin, *W2 = b1 + 32, *b2 = W2 + 32 * 32, *w3 = b2 + 32, *b3 = w3 + 32;
+    double h1[32], h2[32];
+    for (int o = 0; o < 32; ++o) {
+        double s = b1[o];
+        for (int i = 0; i < nin; ++i) s += W1[o * nin + i] * x[i];
+        h1[o] = tanh(s);
+    }
+    for (int o = 0; o < 32; ++o) {
+        double s = b2[o];
+        for (int i = 0; i < 32; ++i) s += W2[o * 32 + i] * h1[i];
+        h2[o] = tanh(s);
+    }
+    double z = b3[0];
+    for (int i = 0; i < 32; ++i) z += w3[i] * h2[i];
+    return 1.0 / (1.0 + exp(-z));
+}
+
+static void modal_features(int Np, const double *Vinv, const int32_t *top, const double *ue, double *uh,
+                           double *S, double *feat)
+{
+    double tot = 0.0, hi = 0.0;
+    for (int i = 0; i < Np; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < Np; ++j) s += Vinv[(long)j * Np + i] * ue[j];
+        uh[i] = s;
+        tot += s * s;
+        if (top[i]) hi += s * s;
+    }
+    *S = tot > 0.0 ? log10(hi / tot) : -INFINITY;
+    if (feat) {
+        const double inv = tot > 0.0 ? 1.0 / sqrt(tot) : 0.0;
+        for (int i = 0; i < Np; ++i) feat[i] = uh[i] * inv;
+    }
+}
+
+void ora_sensor(int Np, const double *Vinv, const int32_t *top, long K, const double *u, double s0, double kappa,
+                double *S, double *sigma, double *feat)
+{
+    double uh[256];
+    for (long e = 0; e < K; ++e) {
+        modal_features(Np, Vinv, top, u + e * Np, uh, &S[e], feat ? feat + e * Np : NULL);
+        sigma[e] = pp_sigma(S[e], s0, kappa);
+    }
+}
+
+void ora_rhs_av(int Np, int Nfp, int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
+                const double *Vinv, const int32_t *top, const int32_t *fmask, long K, const double *u,
+                const double *Rx, const double *Ry, const double *Rz, const double *Sx, const double *Sy,
+                const double *Sz, const double *Tx, const double *Ty, const double *Tz, const double *nx,
+                const double *ny, const double *nz, const double *Fscale, const int64_t *vmapP, int mode, double eps0,
+                double s0, double kappa, const double *mlp, double conf_lo, double conf_hi, double *rhs,
+                double *eps_out, int threads)
+{
+    const int NF = NFACES * Nfp;
+    const double *geo[9] = {Rx, Ry, Rz, Sx, Sy, Sz, Tx, Ty, Tz};
+    const double *nrm[3] = {nx, ny, nz};
+    double *eps = (double *)malloc(sizeof(double) * (size_t)K);
+    double *q = (double *)malloc(sizeof(double) * (size_t)(3 * K * Np));
+    set_threads(threads);
+    /* pass 1: sensor, eps, q */
+#pragma omp parallel for schedule(static) if (threads > 1)
+    for (long e = 0; e < K; ++e) {
+        double uh[256], ft[256], ur[256], us[256], ut[256], fl[3][512];
+        const double *ue = u + e * Np;
+        double S, sig = 0.0;
+        modal_features(Np, Vinv, top, ue, uh, &S, ft);
+        if (mode == 1) {
+            sig = pp_sigma(S, s0, kappa);
+        } else if (mode == 2) {
+            sig = ora_mlp_forward1(Np, mlp, ft);
+            if (sig > conf_lo && sig < conf_hi) sig = pp_sigma(S, s0, kappa);
+        }
+        double fmax = 0.0;
+        for (int m = 0; m < NF; ++m) fmax = fmax > Fscale[e * NF + m] ? fmax : Fscale[e * NF + m];
+        eps[e] = eps0 * sig * (2.0 / fmax) / N;
+        for (int i = 0; i < Np; ++i) {
+            double a = 0.0, b = 0.0, c = 0.0;
+            for (int j = 0; j < Np; ++j) {
+                a += Dr[(long)j * Np + i] * ue[j];
+                b += Ds[(long)j * Np + i] * ue[j];
+                c += Dt[(long)j * Np + i] * ue[j];
+            }
+            ur[i] = a, us[i] = b, ut[i] = c;
+        }
+        for (int m = 0; m < NF; ++m) {
+            const long fid = e * NF + m;
+            const double jump = 0.5 * (u[vmapP[fid]] - ue[fmask[m]]) * Fscale[fid];
+            for (int d = 0; d < 3; ++d) fl[d][m] = nrm[d][fid] * jump;
+        }
+        for (int d = 0; d < 3; ++d)
+            for (int i = 0; i < Np; ++i) {
+                const long idx = e * Np + i;
+                double s = geo[d][idx] * ur[i] + geo[3 + d][idx] * us[i] + geo[6 + d][idx] * ut[i];
+                for (int m = 0; m < NF; ++m) s += LIFT[(long)m * Np + i] * fl[d][m];
+                q[(long)d * K * Np + idx] = s;
+            }
+    }
+    /* pass 2: LF RHS plus the viscous divergence */
+#pragma omp parallel for schedule(static) if (threads > 1)
+    for (long e = 0; e < K; ++e) {
+        double ur[256], us[256], ut[256], flux[512];
+        const double *ue = u + e * Np;
+        for (int i = 0; i < Np; ++i) {
+            double a = 0.0, b = 0.0, c = 0.0;
+            for (int j = 0; j < Np; ++j) {
+                a += Dr[(long)j * Np + i] * ue[j];
+                b += Ds[(long)j * Np + i] * ue[j];
+                c += Dt[(long)j * Np + i] * ue[j];
+            }
+            ur[i] = a, us[i] = b, ut[i] = c;
+        }
+        for (int i = 0; i < Np; ++i) {
+            const long idx = e * Np + i;
+            const double ux = Rx[idx] * ur[i] + Sx[idx] * us[i] + Tx[idx] * ut[i];
+            const double uy = Ry[idx] * ur[i] + Sy[idx] * us[i] + Ty[idx] * ut[i];
+            const double uz = Rz[idx] * ur[i] + Sz[idx] * us[i] + Tz[idx] * ut[i];
+            rhs[idx] = -ue[i] * (ux + uy + uz);
+        }
+        /* eps * sum_d D_d q_d */
+        for (int d = 0; d < 3; ++d) {
+            const double *qd = q + (long)d * K * Np + e * Np;
+            for (int i = 0; i < Np; ++i) {
+                double a = 0.0, b = 0.0, c = 0.0;
+                for (int j = 0; j < Np; ++j) {
+                    a += Dr[(long)j * Np + i] * qd[j];
+                    b += Ds[(long)j * Np + i] * qd[j];
+                    c += Dt[(long)j * Np + i] * qd[j];
+                }
+                const long idx = e * Np + i;
+                rhs[idx] += eps[e] * (geo[d][idx] * a + geo[3 + d][idx] * b + geo[6 + d][idx] * c);
+            }
+        }
+        for (int m = 0; m < NF; ++m) {
+            const long fid = e * NF + m;
+            const long gP = vmapP[fid], gM = e * Np + fmask[m];
+            const double ePs = eps[gP / Np];
+            double vis = 0.0;
+            for (int d = 0; d < 3; ++d)
+                vis += nrm[d][fid] * (ePs * q[(long)d * K * Np + gP] - eps[e] * q[(long)d * K * Np + gM]);
+            flux[m] = lf_surface(u[gM], u[gP], nx[fid] + ny[fid] + nz[fid], Fscale[fid]) + 0.5 * Fscale[fid] * vis;
+        }
+        for (int i = 0; i < Np; ++i) {
+            double s = 0.0;
+            for (int m = 0; m < NF; ++m) s += LIFT[(long)m * Np + i] * flux[m];
+            rhs[e * Np + i] += s;
+        }
+    }
+    if (eps_out) memcpy(eps_out, eps, sizeof(double) * (size_t)K);
+    free(eps);
+    free(q);
+}
+
+long ora_run_av(int Np, int Nfp, int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
+                const double *Vinv, const int32_t *top, const int32_t *fmask, long K, double *u, double *resu,
+                const double *Rx, const double *Ry, const double *Rz, const double *Sx, const double *Sy,
+                const double *Sz, const double *Tx, const double *Ty, const double *Tz, const double *nx,
+                const double *ny, const double *nz, const double *Fscale, const int64_t *vmapP, int mode, double eps0,
+                double s0, double kappa, const double *mlp, double conf_lo, double conf_hi, double dt, int stage0,
+                long nstages, int threads)
+{
+    double *rhs = (double *)calloc((size_t)(K * Np), sizeof(double));
+    for (long s = 0; s < nstages; ++s) {
+        const int st = (int)((stage0 + s) % 5);
+        ora_rhs_av(Np, Nfp, N, Dr, Ds, Dt, LIFT, Vinv, top, fmask, K, u, Rx, Ry, Rz, Sx, Sy, Sz, Tx, Ty, Tz, nx, ny,
+                   nz, Fscale, vmapP, mode, eps0, s0, kappa, mlp, conf_lo, conf_hi, rhs, NULL, threads);
+        lserk_part(K * Np, u, resu, rhs, RK4A[st], RK4B[st], dt);
+    }
+    free(rhs);
+    return nstages;
+}

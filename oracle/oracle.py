@@ -44,6 +44,15 @@ def lib():
                               + [_i64] * 4 + [C.c_double, C.c_int, C.c_long, C.c_int, C.c_int])
         L.ora_run.restype = C.c_long
         L.ora_lserk_coefficients.argtypes = [_d, _d]
+        L.ora_mlp_forward1.argtypes = [C.c_int, _d, _d]
+        L.ora_mlp_forward1.restype = C.c_double
+        L.ora_sensor.argtypes = [C.c_int, _d, _i32, C.c_long, _d, C.c_double, C.c_double, _d, _d, C.c_void_p]
+        av_common = ([C.c_int, C.c_int, C.c_int, _d, _d, _d, _d, _d, _i32, _i32, C.c_long, _d] + [_d] * 13 +
+                     [_i64, C.c_int, C.c_double, C.c_double, C.c_double, C.c_void_p, C.c_double, C.c_double])
+        L.ora_rhs_av.argtypes = av_common[:11] + [_d] + av_common[12:] + [_d, C.c_void_p, C.c_int]
+        L.ora_run_av.argtypes = (av_common[:11] + [_d, _d] + av_common[12:] +
+                                 [C.c_double, C.c_int, C.c_long, C.c_int])
+        L.ora_run_av.restype = C.c_long
         L.ora_max_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -133,3 +142,61 @@ class RunState:
                              u.reshape(-1), resu.reshape(-1), *self.geo, *self.face, self.pick_ptr, self.pick_idx,
                              self.place_ptr, self.place_idx, float(dt), int(stage0), int(nstages), conservative,
                              threads)
+
+
+def mode_degrees(N):
+    """Total degree of every orthonormal mode, modes ordered i, j, k (vandermonde3d.go:15-42)."""
+    return np.array([i + j + k for i in range(N + 1) for j in range(N - i + 1) for k in range(N - i - j + 1)])
+
+
+class AVState:
+    """Artificial-viscosity oracle on one packed mesh (all partitions contiguous; neighbour traces through
+    the global VmapP)."""
+
+    MODES = {"none": 0, "pp": 1, "mlp": 2}
+
+    def __init__(self, prob, eps0=1.0, c0=0.0, kappa=1.0, conf=(0.1, 0.9)):
+        el, geo = prob.el, prob.geo
+        self.prob, self.N, self.Np, self.Nfp, self.K = prob, prob.N, el.Np, el.Nfp, prob.K
+        self.mats = [cm(el.Dr), cm(el.Ds), cm(el.Dt), cm(el.LIFT)]
+        self.vinv = cm(el.Vinv)
+        self.top = np.ascontiguousarray((mode_degrees(prob.N) == prob.N).astype(np.int32))
+        self.fmask = np.ascontiguousarray(el.Fmask.reshape(-1).astype(np.int32))
+        self.geo = [_flat(getattr(geo, n)) for n in ("rx", "ry", "rz", "sx", "sy", "sz", "tx", "ty", "tz")]
+        self.face = [_flat(getattr(geo, n)) for n in ("nx", "ny", "nz", "Fscale")]
+        self.vmapP = np.ascontiguousarray(np.asarray(prob.vmapP, dtype=np.int64).reshape(-1))
+        self.eps0, self.kappa, self.conf = float(eps0), float(kappa), conf
+        self.s0 = -(float(c0) + 4.0 * np.log10(prob.N))
+
+    def _mlp(self, mlp):
+        if mlp is None:
+            return None
+        return np.ascontiguousarray(np.asarray(mlp, dtype=np.float64))
+
+    def sensor(self, u):
+        u = _flat(u)
+        S = np.zeros(self.K)
+        sig = np.zeros(self.K)
+        feat = np.zeros(self.K * self.Np)
+        lib().ora_sensor(self.Np, self.vinv, self.top, self.K, u, self.s0, self.kappa, S, sig,
+                         feat.ctypes.data_as(C.c_void_p))
+        return S, sig, feat.reshape(self.K, self.Np)
+
+    def rhs(self, u, mode="pp", mlp=None, threads=4):
+        u = _flat(u)
+        out = np.zeros_like(u)
+        eps = np.zeros(self.K)
+        m = self._mlp(mlp)
+        lib().ora_rhs_av(self.Np, self.Nfp, self.N, *self.mats, self.vinv, self.top, self.fmask, self.K, u,
+                         *self.geo, *self.face, self.vmapP, self.MODES[mode], self.eps0, self.s0, self.kappa,
+                         None if m is None else m.ctypes.data_as(C.c_void_p), self.conf[0], self.conf[1], out,
+                         eps.ctypes.data_as(C.c_void_p), threads)
+        return out, eps
+
+    def run(self, u, resu, dt, nstages, mode="pp", mlp=None, stage0=0, threads=4):
+        m = self._mlp(mlp)
+        return lib().ora_run_av(self.Np, self.Nfp, self.N, *self.mats, self.vinv, self.top, self.fmask, self.K,
+                                u.reshape(-1), resu.reshape(-1), *self.geo, *self.face, self.vmapP,
+                                self.MODES[mode], self.eps0, self.s0, self.kappa,
+                                None if m is None else m.ctypes.data_as(C.c_void_p), self.conf[0], self.conf[1],
+                                float(dt), int(stage0), int(nstages), threads)
