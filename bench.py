@@ -245,6 +245,46 @@ def run_ensemble(args, world, rank, local):
     E.free()
 
 
+def run_precision(args, world, rank, local):
+    """Config 3: order 7, 32^3 x 6 Kuhn mesh, u0 = 0.5 + 0.25 sin(pi x) cos(pi y) sin(pi z), to t = 0.2: the
+    precision form (tcgen05 BF16 hi/lo GEMMs, FP32 accumulation, compensated FP32 state) against the FP64 run."""
+    import torch
+    from dgkernel_b200.burgers import BurgersProblem, MIXED
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    n = 32 if args.n == 64 else args.n
+    res = {}
+    for name, dt in (("f64", np.float64), ("tc", MIXED)):
+        P = BurgersProblem(7, n, 1, dt, "smooth", stream=stream.cuda_stream, tensor=True if dt == MIXED else None)
+        nst = 5 * int(np.ceil(0.2 / P.dt))
+        P.run_stages(args.warmup)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            P.run_stages(nst - args.warmup)
+            e1.record(stream)
+            torch.cuda.synchronize()
+        res[name] = {"ms": e0.elapsed_time(e1) / (nst - args.warmup), "u": P.get("u"), "dofs": P.dofs,
+                     "stages": nst, "clk": clk.summary()}
+        P.free()
+    ref, tc = res["f64"]["u"], res["tc"]["u"]
+    l2 = float(np.linalg.norm(tc - ref) / np.linalg.norm(ref))
+    linf = float(np.max(np.abs(tc - ref)) / np.max(np.abs(ref)))
+    if rank == 0:
+        m = res["tc"]
+        out = {"metric": "DOF-stage-updates/s, precision form (config 3)", "value": world * m["dofs"] / (m["ms"] * 1e-3),
+               "unit": UNIT, "n_gpus": world, "steps": m["stages"], "warmup": args.warmup, "ms_per_step": m["ms"],
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3 (fp32 acc)",
+               "data": "synthetic",
+               "config": {"workload": f"3-D Burgers, order 7 (Np=120), periodic {n}^3x6 Kuhn mesh, u0 = 0.5 + 0.25 "
+                                      f"sin cos sin, to t = 0.2", "l2_err_vs_fp64": l2, "linf_err_vs_fp64": linf,
+                          "fp64_ms_per_step": res["f64"]["ms"],
+                          "fp64_value": world * m["dofs"] / (res["f64"]["ms"] * 1e-3)},
+               "clocks": m["clk"], "gpu_launches": m["stages"]}
+        print(json.dumps(out), flush=True)
+
+
 def run_learned(args, world, rank, local):
     """Config 5: shock-forming u0 = 0.5 + sin sin sin, order 4, 48^3 x 6, to t = 0.5 with artificial viscosity.
     The sensor network is trained first (library kernels) on (modal features, PP activation) pairs from PP
@@ -324,8 +364,8 @@ def main():
     ap.add_argument("--slabs", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="burgers", choices=["burgers", "ensemble", "learned"],
-                    help="burgers: config 2 (default); ensemble: config 4 batching form; learned: config 5")
+    ap.add_argument("--workload", default="burgers", choices=["burgers", "ensemble", "learned", "precision"],
+                    help="burgers: config 2 (default); precision: config 3; ensemble: config 4; learned: config 5")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
@@ -340,6 +380,8 @@ def main():
         return run_ensemble(args, world, rank, local)
     if args.workload == "learned":
         return run_learned(args, world, rank, local)
+    if args.workload == "precision":
+        return run_precision(args, world, rank, local)
     import torch
     from dgkernel_b200.burgers import BurgersProblem, RK4A, RK4B, MIXED
     torch.cuda.set_device(local)

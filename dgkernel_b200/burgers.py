@@ -208,6 +208,8 @@ class _TetBurgers:
         if not self.mixed:
             return f"rhsStage(conservative={self.conservative})"
         args = [f"conservative={self.conservative}"]
+        if getattr(self, "tensor", None) is not None:
+            args.append(f"tensor={int(self.tensor)}")
         if warps:
             args.append(f"warps={warps}")
         if ring:
@@ -297,8 +299,9 @@ class BurgersProblem(_TetBurgers):
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
                  cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None,
                  viscosity=None, eps0: float = 1.0, c0: float = 0.0, kappa: float = 1.0, conf=(0.1, 0.9),
-                 mode_sigma: float = 0.1):
+                 mode_sigma: float = 0.1, tensor=None):
         self.n, self.nslab = n, nslab
+        self.tensor = tensor  # mixed form: None = by order (tensor cores for orders 6, 7), True / False to force
         VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)
         EToE, EToF = M.ti_connect3d(EToVp)
         K = EToV.shape[0]

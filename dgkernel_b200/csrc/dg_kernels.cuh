@@ -145,6 +145,28 @@ struct SplitJoinArgs {
   float *hi, *lo;
 };
 
+// ---- precision form on the tensor cores (tc.cu) ----
+struct TcArgs {
+  const MTile *tiles;  // tiles of up to 64 elements; elem_slot indexes the compact geometry / connectivity
+  int ntiles;
+  const float *uhi_in, *ulo_in;
+  float *uhi_out, *ulo_out, *resu;
+  const float *geo;          // kMixedGeoWords per element slot
+  const int32_t *conn;       // kMixedConnWords per element slot
+  int64_t n_u_values;
+  const unsigned char *amat; // Dr, Ds, Dt, LIFT as BF16 hi/lo in the canonical K-major layout
+  int64_t aoff[4];           // byte offsets of the four matrices in amat
+  const double *bary;        // [NP][3]
+  const int32_t *vtx;        // vertex nodes A..D
+  const uint8_t *ftab;
+  const int32_t *fmask;
+  int ncodes;
+  float a, dt;
+  double b;
+  int conservative;
+  int *status;
+};
+
 // ---- artificial-viscosity stage and shock-sensor MLP (av.cu) ----
 struct AvTile {
   int64_t node_base;  // value index of the tile's first element in node arrays

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "dg_kernels.cuh"
 
 namespace dgk {
@@ -36,6 +38,12 @@ uint32_t mixed_slot_bytes(int N);  // 0 when the order has no such form
 template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);
 void launch_split_join(const SplitJoinArgs &a, cudaStream_t st);
+
+// Precision form on the tensor cores (tc.cu): orders 4..7.
+bool launch_rhs_tc(int N, const TcArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info);
+int tc_tile_elems();
+void tc_pack_operands(const double *const *mats, const int *cols, int rows, std::vector<uint16_t> &out,
+                      int64_t off[4]);
 
 // Artificial-viscosity stage and the sensor MLP (av.cu).
 void launch_av(int N, const AvArgs &A, int num_sms, cudaStream_t st);

@@ -382,9 +382,10 @@ struct MatmulOp : Op {
 // nz, Fscale (float64 or float32, read at build time only); gmap (int32, value indices into uhi's layout);
 // matrices Dr, Ds, Dt, LIFT, Fmask and Bary (Np x 4 barycentric coordinates of the nodes).
 struct MixedOp : Op {
-  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0;
+  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0, tensor = 0;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
-  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask;
+  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat;
+  int64_t aoff[4] = {0, 0, 0, 0};
   LaunchInfo info;
 
   template <typename G>
@@ -419,7 +420,7 @@ struct MixedOp : Op {
     cuda_check(cudaStreamSynchronize(r.stream()), "compact geometry");
     if (bad)
       throw Error(DGK_ERR_UNSUPPORTED, kname + ": the mixed stage needs straight-sided elements; " + std::to_string(bad) +
-                                           " elements have non-constant metrics or face factors");
+                                           " elements have metrics or face factors that vary by more than 1e-6");
   }
 
   MixedOp(Runner &r, Roles &R) {
@@ -445,7 +446,11 @@ struct MixedOp : Op {
             *fm = R.matrix("Fmask"), *B = R.matrix("Bary");
     const int64_t np = Dr->rows;
     N = order_from_np(np);
-    if (mixed_slot_bytes(N) == 0)
+    // orders 6 and 7 (and any order with tensor=1) run the precision form on the tensor cores
+    tensor = R.flag("tensor", N >= 6 ? 1 : 0);
+    if (tensor && (N < 4 || N > 7))
+      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the tensor-core form is built for orders 4..7");
+    if (!tensor && mixed_slot_bytes(N) == 0)
       throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the mixed stage is built for orders 1..5");
     const int nfp = (N + 1) * (N + 2) / 2, nf = 4 * nfp;
     require(uhi->values_per_elem == np, R.kname + ": uhi must hold Np values per element");
@@ -516,24 +521,64 @@ struct MixedOp : Op {
     std::vector<int32_t> fmi(fm->mat.begin(), fm->mat.end());
     for (int32_t v : fmi) require(v >= 0 && v < np, R.kname + ": Fmask entry out of range");
     fmask.upload(fmi.data(), fmi.size() * sizeof(int32_t));
+    if (tensor) {  // BF16 hi/lo operands of Dr, Ds, Dt and LIFT in the tensor cores' canonical layout
+      const double *mats[4] = {Dr->mat.data(), Ds->mat.data(), Dt->mat.data(), L->mat.data()};
+      const int cols[4] = {(int)np, (int)np, (int)np, nf};
+      std::vector<uint16_t> packed;
+      tc_pack_operands(mats, cols, (int)np, packed, aoff);
+      amat.upload(packed.data(), packed.size() * sizeof(uint16_t));
+    }
+    const int te = tensor ? tc_tile_elems() : kMixedSlotElems;
     std::vector<MTile> tl;
     for (int p = 0; p < P; ++p)
-      for (int64_t s0 = 0; s0 < r.K[p]; s0 += kMixedSlotElems) {
+      for (int64_t s0 = 0; s0 < r.K[p]; s0 += te) {
         MTile x;
         x.node_base = uhi->offsets[p] + s0 * np;
         x.elem_slot = slot_prefix[p] + s0;
-        x.nelem = (int32_t)std::min<int64_t>(kMixedSlotElems, r.K[p] - s0);
+        x.nelem = (int32_t)std::min<int64_t>(te, r.K[p] - s0);
         x.part = p;
-        require((x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
+        require(tensor || (x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
         tl.push_back(x);
       }
     ntiles = (int)tl.size();
     tiles.upload(tl.data(), std::max<size_t>(tl.size(), 1) * sizeof(MTile));
   }
   std::vector<std::string> scalar_names() const override { return {"a", "b", "dt"}; }
-  void prepare(Runner &) override { prepare_rhs_mixed(N, warps); }
+  void prepare(Runner &) override {
+    if (!tensor) prepare_rhs_mixed(N, warps);
+  }
+  void launch_tensor(Runner &r, const std::vector<double> &s) {
+    TcArgs A{};
+    A.tiles = tiles.get<MTile>();
+    A.ntiles = ntiles;
+    A.uhi_in = reinterpret_cast<const float *>(uhi->dptr);
+    A.ulo_in = reinterpret_cast<const float *>(ulo->dptr);
+    A.uhi_out = reinterpret_cast<float *>(uhin->dptr);
+    A.ulo_out = reinterpret_cast<float *>(ulon->dptr);
+    A.resu = reinterpret_cast<float *>(resu->dptr);
+    A.geo = geoE.get<float>();
+    A.conn = conn.get<int32_t>();
+    A.n_u_values = uhi->offsets.back();
+    A.amat = amat.get<unsigned char>();
+    for (int c = 0; c < 4; ++c) A.aoff[c] = aoff[c];
+    A.bary = bary.get<double>();
+    A.vtx = vtx.get<int32_t>();
+    A.ftab = ftab.get<uint8_t>();
+    A.fmask = fmask.get<int32_t>();
+    A.ncodes = ncodes;
+    A.a = (float)s[0];
+    A.b = s[1];
+    A.dt = (float)s[2];
+    A.conservative = conservative;
+    A.status = r.status_word();
+    if (!launch_rhs_tc(N, A, r.num_sms, r.stream(), &info))
+      throw Error(DGK_ERR_UNSUPPORTED, "tensor-core stage: no form for this order");
+    std::swap(uhi->dptr, uhin->dptr);
+    std::swap(ulo->dptr, ulon->dptr);
+  }
   void launch(Runner &r, const std::vector<double> &s) override {
     if (ntiles == 0) return;
+    if (tensor) return launch_tensor(r, s);
     MixedArgs A{};
     A.tiles = tiles.get<MTile>();
     A.ntiles = ntiles;
