@@ -334,16 +334,17 @@ def run_learned(args, world, rank, local):
         P.run_stages(args.warmup)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        P.run_stages(nst - args.warmup)
-        e1.record(stream)
-        torch.cuda.synchronize()
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            P.run_stages(nst - args.warmup)
+            e1.record(stream)
+            torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / (nst - args.warmup)
         fb = None
         if sensor == "mlp":
             _, sg, mo = P.sensor_features("mlp")
             fb = float(((mo > 0.1) & (mo < 0.9)).mean())
-        runs[sensor] = {"u": P.get("u"), "ms": ms, "dofs": P.dofs, "stages": nst, "fallback": fb}
+        runs[sensor] = {"u": P.get("u"), "ms": ms, "dofs": P.dofs, "stages": nst, "fallback": fb, "clk": clk.summary()}
         P.free()
     ref = runs["pp"]["u"]
     finite = {k: bool(np.isfinite(v["u"]).all()) for k, v in runs.items()}
@@ -360,7 +361,7 @@ def run_learned(args, world, rank, local):
                           "fallback_fraction_at_t_final": m["fallback"], "training_pairs": npairs,
                           "active_fraction": active, "balanced_pairs": int(len(Yb)), "train_loss": [hist[0], hist[-1]],
                           "data_s": data_s, "train_s": train_s},
-               "gpu_launches": 2 * m["stages"]}
+               "clocks": m["clk"], "gpu_launches": 2 * m["stages"]}
         print(json.dumps(out), flush=True)
 
 
