@@ -111,8 +111,11 @@ def dist_setup(args):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        else:  # host-only ranks (the reference arm's plumbing, tests): gloo
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
     return world, rank, local
 
 
@@ -121,7 +124,8 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -145,44 +149,29 @@ def time_stages(prob, steps: int, stream):
     return e0.elapsed_time(e1) / steps  # ms per stage
 
 
-def cpu_baseline(N: int, steps: int, seconds: float = 12.0):
+def cpu_baseline(N: int, steps: int, seconds: float = 12.0, n: int = 16):
     """Oracle port (C restatement of the OKL loops, OpenMP over the @outer partition loop) on a bounded
-    sample of the same workload: order N, 16 x-slab partitions of a 16^3 x 6 Kuhn mesh (24,576 tets)."""
+    sample of the same workload: order N, 16 x-slab partitions of an n^3 x 6 Kuhn mesh (n = 16: 24,576 tets),
+    set up by the oracle's own numpy restatement of the reference's setup chain (no GPU involved)."""
+    from oracle import burgers_ref as BR
     from oracle import oracle as O
-    from dgkernel_b200.burgers import BurgersProblem, GEO, FACE
-    from dgkernel_b200 import mesh as M
-    prob = BurgersProblem(N, 16, 16, np.float64, "modes")
-    el = prob.el
-    geo = [prob.get(nm) for nm in GEO]
-    face = [prob.get(nm) for nm in FACE]
-    fc = M.FaceConnector(prob.K, 4, el.Nfp, el.Np, prob.vmapP, prob.EToP)
-    P = fc.NumPartitions
-    pick_ptr, pick_idx = O.csr_pairs(fc.pick, P)
-    place_ptr, place_idx = O.csr_pairs(fc.place, P)
-    K = np.asarray(prob.Kpart, dtype=np.int64)
-    noff = np.concatenate(([0], np.cumsum(K * el.Np))).astype(np.int64)
-    foff = np.concatenate(([0], np.cumsum(K * 4 * el.Nfp))).astype(np.int64)
-    mats = [O.cm(el.Dr), O.cm(el.Ds), O.cm(el.Dt), O.cm(el.LIFT)]
-    fmask = np.ascontiguousarray(el.Fmask.reshape(-1).astype(np.int32))
-    u = np.ascontiguousarray(prob.u0.astype(np.float64))
+    ref = BR.Problem(N, n, 16, "modes")
+    rs = O.RunState(ref)
+    u = np.ascontiguousarray(ref.u0, dtype=np.float64).copy()
     resu = np.zeros_like(u)
-    dt = prob.dt
-    prob.free()
+    P = len(rs.K)
     threads = max(1, min(os.cpu_count() or 1, P))
-    L = O.lib()
-    args = (el.Np, el.Nfp, *mats, fmask, P, K, noff, foff, u, resu, *geo, *face, pick_ptr, pick_idx, place_ptr,
-            place_idx, float(dt))
-    L.ora_run(*args, 0, 1, 0, threads)  # warm-up stage
+    rs.run(u, resu, ref.dt, 1, 0, 0, threads)  # warm-up stage
     done, t0 = 0, time.perf_counter()
     while True:
-        L.ora_run(*args, done % 5, 1, 0, threads)
+        rs.run(u, resu, ref.dt, 1, done % 5, 0, threads)
         done += 1
         el_t = time.perf_counter() - t0
         if (steps and done >= steps) or (not steps and el_t >= seconds):
             break
-    value = prob.dofs * done / el_t
+    value = u.size * done / el_t
     return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"order {N}, 16^3x6 Kuhn mesh (24,576 tets, {P} x-slab partitions), {done} LSERK4 stages of "
+            "sample": f"order {N}, {n}^3x6 Kuhn mesh ({ref.K:,} tets, {P} x-slab partitions), {done} LSERK4 stages of "
                       f"exchange + LF RHS + update, C restatement of the OKL loops (gcc -O3 -fopenmp, "
                       f"-ffp-contract=off), OpenMP over partitions, {threads} threads of {os.cpu_count()} host cores",
             "seconds": el_t}
@@ -381,19 +370,24 @@ def main():
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
-    if args.impl == "reference":
-        run_reference(args, world, rank)
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        if args.workload == "ensemble":
+            return run_ensemble(args, world, rank, local)
+        if args.workload == "learned":
+            return run_learned(args, world, rank, local)
+        if args.workload == "precision":
+            return run_precision(args, world, rank, local)
+        return run_burgers(args, world, rank, local)
+    finally:
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
-        return
 
-    if args.workload == "ensemble":
-        return run_ensemble(args, world, rank, local)
-    if args.workload == "learned":
-        return run_learned(args, world, rank, local)
-    if args.workload == "precision":
-        return run_precision(args, world, rank, local)
+
+def run_burgers(args, world, rank, local):
+    """Config 2 (the default line): plain FP64, plain FP32 and mixed forms from one u0; the chosen form."""
     import torch
     from dgkernel_b200.burgers import BurgersProblem, RK4A, RK4B, MIXED
     torch.cuda.set_device(local)
@@ -502,9 +496,6 @@ def main():
             "gpu_launches": args.steps,
         }
         print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
 
 
 if __name__ == "__main__":
