@@ -210,6 +210,8 @@ class _TetBurgers:
         args = [f"conservative={self.conservative}"]
         if getattr(self, "tensor", None) is not None:
             args.append(f"tensor={int(self.tensor)}")
+        if getattr(self, "mma", None):
+            args.append("mma=1")
         if warps:
             args.append(f"warps={warps}")
         if ring:
@@ -299,9 +301,10 @@ class BurgersProblem(_TetBurgers):
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
                  cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None,
                  viscosity=None, eps0: float = 1.0, c0: float = 0.0, kappa: float = 1.0, conf=(0.1, 0.9),
-                 mode_sigma: float = 0.1, tensor=None):
+                 mode_sigma: float = 0.1, tensor=None, mma=None):
         self.n, self.nslab = n, nslab
         self.tensor = tensor  # mixed form: None = by order (tensor cores for orders 6, 7), True / False to force
+        self.mma = mma  # mixed form, orders 1..4: element-local products on the tensor cores (3-part BF16)
         VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)
         EToE, EToF = M.ti_connect3d(EToVp)
         K = EToV.shape[0]
@@ -324,8 +327,9 @@ class BurgersEnsemble(_TetBurgers):
     seed + i; all instances share one time step, the CFL step of the most restrictive one."""
 
     def __init__(self, N: int, sizes, dtype=MIXED, seed: int = DEFAULT_SEED, cfl: float = 0.3, conservative: int = 0,
-                 stream=None, warps=None, ring=None):
+                 stream=None, warps=None, ring=None, mma=None):
         self.sizes = [int(n) for n in sizes]
+        self.mma = mma
         VX, VY, VZ, EToV, EToE, EToF, EToP = _concat_meshes(self.sizes)
         Kpart = [6 * n ** 3 for n in self.sizes]
         self._assemble(N, VX, VY, VZ, EToV, EToE, EToF, EToP, Kpart, dtype, stream)

@@ -113,6 +113,7 @@ struct MixedArgs {
   int64_t n_u_values;            // bound of every gathered value index
   const float *Dm;               // [NP][NPJ][3]: Dr, Ds, Dt entries interleaved per column, zero-padded
   const float *lift;             // [NP][4 Nfp]
+  const unsigned char *bmat;     // tensor-core form: split BF16 operands of D and LIFT (tcm_pack_operands)
   const double *bary;            // [NP][3] barycentric weights of vertices B, C, D at each node
   const int32_t *vtx;            // node index of vertices A, B, C, D
   const uint8_t *ftab;           // [ncodes][Nfp] neighbour-local node index of each face point

@@ -35,6 +35,15 @@ bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int ring_ma
                       LaunchInfo *info);
 void prepare_rhs_mixed(int N, int consumer_warps);  // attributes, before any stream capture
 uint32_t mixed_slot_bytes(int N);  // 0 when the order has no such form
+// Mixed stage with the element-local products on the tensor cores (tcm.cu), orders 1..4: tiles of
+// tcm_tile_elems() elements; the operand buffer comes from tcm_pack_operands (Dr, Ds, Dt, LIFT row-major FP64).
+bool tcm_supported(int N);
+int tcm_tile_elems();
+void tcm_pack_operands(int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
+                       std::vector<uint16_t> &out);
+// consumer_warps 8 or 16 (2 or 4 threads per element)
+void prepare_rhs_tcm(int N, int consumer_warps);  // attributes, before any stream capture
+bool launch_rhs_tcm(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st, LaunchInfo *info);
 template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);
 void launch_split_join(const SplitJoinArgs &a, cudaStream_t st);

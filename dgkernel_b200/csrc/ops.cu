@@ -382,9 +382,9 @@ struct MatmulOp : Op {
 // nz, Fscale (float64 or float32, read at build time only); gmap (int32, value indices into uhi's layout);
 // matrices Dr, Ds, Dt, LIFT, Fmask and Bary (Np x 4 barycentric coordinates of the nodes).
 struct MixedOp : Op {
-  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0, tensor = 0;
+  int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0, tensor = 0, mma = 0;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
-  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat;
+  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat, bmat;
   int64_t aoff[4] = {0, 0, 0, 0};
   LaunchInfo info;
 
@@ -427,8 +427,6 @@ struct MixedOp : Op {
     static const char *gn[9] = {"Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz"};
     static const char *fn[4] = {"nx", "ny", "nz", "Fscale"};
     conservative = R.flag("conservative", 0);
-    warps = R.flag("warps", 11);
-    require(warps == 4 || warps == 8 || warps == 11, R.kname + ": warps must be 4, 8 or 11");
     ring = R.flag("ring", 0);
     require(ring == 0 || (ring >= 2 && ring <= 24), R.kname + ": ring must be 0 (fill shared memory) or 2..24");
     uhi = R.array("uhi");
@@ -452,6 +450,17 @@ struct MixedOp : Op {
       throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the tensor-core form is built for orders 4..7");
     if (!tensor && mixed_slot_bytes(N) == 0)
       throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the mixed stage is built for orders 1..5");
+    // mma=1: the element-local products on the tensor cores with three-part BF16 operands (orders 1..4)
+    mma = tensor ? 0 : R.flag("mma", 0);
+    if (mma && !tcm_supported(N))
+      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the tensor-core mixed stage is built for orders 1..4");
+    if (mma) {
+      warps = R.flag("warps", 16);
+      require(warps == 8 || warps == 16, R.kname + ": warps must be 8 or 16 with mma=1");
+    } else {
+      warps = R.flag("warps", 11);
+      require(warps == 4 || warps == 8 || warps == 11, R.kname + ": warps must be 4, 8 or 11");
+    }
     const int nfp = (N + 1) * (N + 2) / 2, nf = 4 * nfp;
     require(uhi->values_per_elem == np, R.kname + ": uhi must hold Np values per element");
     for (Binding *m : {Dr, Ds, Dt}) require(m->rows == np && m->cols == np, R.kname + ": " + m->name + " must be Np x Np");
@@ -528,7 +537,12 @@ struct MixedOp : Op {
       tc_pack_operands(mats, cols, (int)np, packed, aoff);
       amat.upload(packed.data(), packed.size() * sizeof(uint16_t));
     }
-    const int te = tensor ? tc_tile_elems() : kMixedSlotElems;
+    if (mma) {
+      std::vector<uint16_t> packed;
+      tcm_pack_operands(N, Dr->mat.data(), Ds->mat.data(), Dt->mat.data(), L->mat.data(), packed);
+      bmat.upload(packed.data(), packed.size() * sizeof(uint16_t));
+    }
+    const int te = tensor ? tc_tile_elems() : mma ? tcm_tile_elems() : kMixedSlotElems;
     std::vector<MTile> tl;
     for (int p = 0; p < P; ++p)
       for (int64_t s0 = 0; s0 < r.K[p]; s0 += te) {
@@ -545,7 +559,10 @@ struct MixedOp : Op {
   }
   std::vector<std::string> scalar_names() const override { return {"a", "b", "dt"}; }
   void prepare(Runner &) override {
-    if (!tensor) prepare_rhs_mixed(N, warps);
+    if (mma)
+      prepare_rhs_tcm(N, warps);
+    else if (!tensor)
+      prepare_rhs_mixed(N, warps);
   }
   void launch_tensor(Runner &r, const std::vector<double> &s) {
     TcArgs A{};
@@ -602,6 +619,14 @@ struct MixedOp : Op {
     A.dt = (float)s[2];
     A.conservative = conservative;
     A.status = r.status_word();
+    if (mma) {
+      A.bmat = bmat.get<unsigned char>();
+      if (!launch_rhs_tcm(N, A, warps, r.num_sms, r.stream(), &info))
+        throw Error(DGK_ERR_UNSUPPORTED, "tensor-core mixed stage: shared memory does not fit this order");
+      std::swap(uhi->dptr, uhin->dptr);
+      std::swap(ulo->dptr, ulon->dptr);
+      return;
+    }
     if (!launch_rhs_mixed(N, A, warps, ring, r.num_sms, r.stream(), &info))
       throw Error(DGK_ERR_UNSUPPORTED, "mixed stage: no launch shape fits shared memory for this order");
     std::swap(uhi->dptr, uhin->dptr);  // "uhi"/"ulo" always name the newest state

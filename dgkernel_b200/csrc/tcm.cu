@@ -1,0 +1,518 @@
+// Mixed-precision stage with its element-local products on the tensor cores (tcgen05, sm_100a), orders 1..4.
+//
+// Same arithmetic contract as rhs_stage_mixed_kernel (mixed.cu): the state is a compensated FP32 pair
+// (u = hi + lo), the residual FP32, the update FP64; the derivative operand is w minus its linear vertex
+// interpolant (w = u or u^2/2), whose exact derivative is added back; the Lax-Friedrichs flux is formed in
+// FP32.  The two products per element, D{r,s,t} dw and LIFT flux, run as GEMMs over tiles of 128 elements:
+//
+//   acc_V[e][3i+d] = sum_j dw[e][j] D_d[i][j]      M = 128 elements, N = rup16(3 Np), K = rup16(Np)
+//   acc_L[e][i]    = sum_m fl[e][m] LIFT[i][m]     M = 128 elements, N = rup16(Np),   K = rup16(4 Nfp)
+//
+// with elements on the MMA's M dimension, so that TMEM lane e holds element e's outputs and the threads that
+// own element e read them back.  Every operand is split into three BF16 parts, x = x0 + x1 + x2 (x0 = bf16(x),
+// x1 = bf16(x - x0), x2 = bf16(x - x0 - x1), about 24 significant bits), and a product keeps the six terms
+// a_p b_q with p + q <= 2, all accumulated in one FP32 TMEM accumulator: the products carry FP32-level
+// rounding (the dropped terms are below 2^-24 of the product).
+//
+// CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry and connectivity into a
+// 2-slot ring with 1-D bulk copies; CW consumer warps hold CW / 4 threads per element (warps w, w + 4, ... share
+// the TMEM lane quarter w mod 4 and split the element's nodes and face points in 8-wide chunks).  Per tile: the
+// threads write the split dw into the A buffer (K-major canonical layout), one thread issues the volume MMAs,
+// the threads gather the neighbour traces and form the flux meanwhile, write it into the same A buffer once
+// the volume MMAs have completed, one thread issues the LIFT MMAs, and the threads read both accumulators from
+// TMEM, finish the stage in FP64 and write the slot back with bulk stores.  Constant operands (D and LIFT,
+// split) stay in shared memory for the whole launch.  Every wait is bounded; a failed wait sets the status
+// word and the CTA leaves after draining its copies and MMAs; TMEM is always freed.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdint>
+
+#include "dg_kernels.cuh"
+#include "kernels.hpp"
+#include "runner.hpp"
+#include "tcgen05.cuh"
+#include "tma.cuh"
+
+namespace dgk {
+
+namespace {
+
+constexpr int kTmTE = 128;    // elements per tile (the MMA's M)
+constexpr int kTmCols = 256;  // TMEM columns (volume and LIFT accumulators)
+
+template <int N>
+struct TmCfg {
+  using O = Order<N>;
+  static constexpr int NP = O::NP, NFP = O::NFP, NF = O::NF;
+  static constexpr int KV = rup16(NP), KL = rup16(NF), NV = rup16(3 * NP), NL = rup16(NP);
+  static constexpr int KA = KV > KL ? KV : KL;
+  static constexpr uint32_t BV_PART = (uint32_t)NV * KV * 2, BL_PART = (uint32_t)NL * KL * 2;
+  static constexpr uint32_t A_PART = (uint32_t)kTmTE * KA * 2;
+  static constexpr uint32_t NODE_B = (uint32_t)kTmTE * NP * 4;
+  static constexpr uint32_t GEO_B = (uint32_t)kTmTE * kMixedGeoWords * 4;
+  static constexpr uint32_t CONN_B = (uint32_t)kTmTE * kMixedConnWords * 4;
+  static constexpr uint32_t SLOT_B = 3 * NODE_B + GEO_B + CONN_B;
+  // shared-memory layout (bytes)
+  static constexpr uint32_t OFF_BV = 0, OFF_BL = OFF_BV + 3 * BV_PART, OFF_A = OFF_BL + 3 * BL_PART;
+  static constexpr uint32_t OFF_SLOT = OFF_A + 3 * A_PART, OFF_BARY = OFF_SLOT + 2 * SLOT_B;
+  static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;  // full[2], empty[2], vol, lift
+  static constexpr uint32_t OFF_MISC = OFF_BARS + 6 * 8;                  // abort flag, TMEM base
+  static constexpr uint32_t OFF_FMASK = OFF_MISC + 16;
+  static constexpr uint32_t OFF_FTAB = OFF_FMASK + ((NF + 15) & ~15);
+  static constexpr uint32_t CONST_BYTES = 3 * BV_PART + 3 * BL_PART;  // the packed operand buffer
+  static_assert(3 * NP <= 256 && NP <= 128, "tile shapes");
+};
+
+template <int N>
+__host__ __device__ constexpr uint32_t tm_smem(int ncodes) {
+  return TmCfg<N>::OFF_FTAB + (((uint32_t)ncodes * TmCfg<N>::NFP + 15u) & ~15u);
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
+         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+}
+
+// Split 8 values into three BF16 parts and store each part's 16 bytes at `dst + p * part_bytes`.
+__device__ __forceinline__ void store_split8(unsigned char *dst, uint32_t part_bytes, const float (&v)[8]) {
+  float r1[8], r2[8];
+  uint32_t w0[4], w1[4], w2[4];
+#pragma unroll
+  for (int q = 0; q < 8; ++q) {
+    const float x0 = __bfloat162float(__float2bfloat16_rn(v[q]));
+    r1[q] = v[q] - x0;
+    const float x1 = __bfloat162float(__float2bfloat16_rn(r1[q]));
+    r2[q] = r1[q] - x1;
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    w0[q] = pack_bf16(v[2 * q], v[2 * q + 1]);
+    w1[q] = pack_bf16(r1[2 * q], r1[2 * q + 1]);
+    w2[q] = pack_bf16(r2[2 * q], r2[2 * q + 1]);
+  }
+  *reinterpret_cast<uint4 *>(dst) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
+  *reinterpret_cast<uint4 *>(dst + part_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
+  *reinterpret_cast<uint4 *>(dst + 2 * part_bytes) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
+}
+
+// bar.red.or over the CW consumer warps (named barrier 1): every consumer thread gets the same answer.
+template <int CW>
+__device__ __forceinline__ bool consumers_any(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "n"(32 * CW)
+      : "memory");
+  return r != 0;
+}
+
+// Four 8-column TMEM loads of this warp's lanes under one wait.
+__device__ __forceinline__ void tmem_ld8x4(uint32_t t0, uint32_t t1, uint32_t t2, uint32_t t3, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%33];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16,%17,%18,%19,%20,%21,%22,%23}, [%34];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%24,%25,%26,%27,%28,%29,%30,%31}, [%35];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(t0), "r"(t1), "r"(t2), "r"(t3)
+      : "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// One GEMM of the split products: 6 MMAs per 16-wide K step into the accumulator at `acc`.
+__device__ __forceinline__ void split_gemm(uint32_t acc, uint32_t a0, uint32_t a_part, uint32_t b0, uint32_t b_part,
+                                           int K, int NB, uint32_t idesc) {
+  const int pa[6] = {0, 0, 1, 0, 2, 1}, pb[6] = {0, 1, 0, 2, 0, 1};
+  for (int ks = 0; ks < K / 16; ++ks) {
+    const uint32_t ao = (uint32_t)ks * 2 * (kTmTE / 8) * 128, bo = (uint32_t)ks * 2 * (NB / 8) * 128;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      const uint64_t da = smem_desc(a0 + pa[t] * a_part + ao, (kTmTE / 8) * 128, 128);
+      const uint64_t db = smem_desc(b0 + pb[t] * b_part + bo, (NB / 8) * 128, 128);
+      tc_mma(acc, da, db, idesc, (ks > 0 || t > 0) ? 1u : 0u);
+    }
+  }
+}
+
+__device__ __forceinline__ int vload(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
+
+}  // namespace
+
+// CW = 8 or 16 consumer warps: CW / 4 threads per element.
+template <int N, int CW>
+__global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const MixedArgs A) {
+  using C = TmCfg<N>;
+  constexpr int TPE = CW / 4;  // threads per element
+  constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, KV = C::KV, KL = C::KL, NV = C::NV, NL = C::NL;
+  constexpr int TE = kTmTE;
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char *sBV = sm + C::OFF_BV, *sBL = sm + C::OFF_BL, *sA = sm + C::OFF_A;
+  unsigned char *ring = sm + C::OFF_SLOT;
+  double *sBary = reinterpret_cast<double *>(sm + C::OFF_BARY);
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *empty = full + 2, *mvol = full + 4,
+           *mlift = full + 5;
+  int *sMisc = reinterpret_cast<int *>(sm + C::OFF_MISC);  // [0] abort flag, [1] TMEM base
+  uint8_t *sFm = sm + C::OFF_FMASK, *sFt = sm + C::OFF_FTAB;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int G = gridDim.x;
+
+  // constant operands, tables and barriers
+  {
+    const uint4 *src = reinterpret_cast<const uint4 *>(A.bmat);
+    uint4 *dst = reinterpret_cast<uint4 *>(sBV);
+    for (int x = tid; x < (int)(C::CONST_BYTES / 16); x += blockDim.x) dst[x] = src[x];
+  }
+  for (int x = tid; x < NP * 3; x += blockDim.x) sBary[x] = A.bary[x];
+  for (int x = tid; x < NF; x += blockDim.x) sFm[x] = (uint8_t)A.fmask[x];
+  for (int x = tid; x < A.ncodes * NFP; x += blockDim.x) sFt[x] = A.ftab[x];
+  if (tid == 0) {
+    for (int b = 0; b < 6; ++b) mbar_init(&full[b], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    sMisc[0] = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&sMisc[1])),
+                 "r"(kTmCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_async_smem();  // the constant operands are read by the tensor cores (async proxy)
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = (uint32_t)sMisc[1];
+
+  if (warp == CW) {  // producer: lane 0 streams this CTA's tiles through the 2-slot ring
+    if (lane == 0) {
+      int k = 0;
+      bool bad = false;
+      for (;; ++k) {
+        const int t = blockIdx.x + k * G;
+        if (t >= A.ntiles) break;
+        const int s = k & 1;
+        if (k >= 2 && !mbar_wait_bounded(&empty[s], (uint32_t)((k >> 1) - 1) & 1u, kSpinLimit)) {
+          bad = true;
+          break;
+        }
+        if (vload(&sMisc[0])) {
+          bad = true;
+          break;
+        }
+        const MTile tl = A.tiles[t];
+        unsigned char *slot = ring + (size_t)s * C::SLOT_B;
+        const uint32_t nb = round16((uint32_t)(tl.nelem * NP * 4));
+        const uint32_t gb = (uint32_t)tl.nelem * kMixedGeoWords * 4;
+        const uint32_t cb = round16((uint32_t)(tl.nelem * kMixedConnWords * 4));
+        mbar_expect_tx(&full[s], 3 * nb + gb + cb);
+        bulk_g2s(slot, A.uhi_in + tl.node_base, nb, &full[s]);
+        bulk_g2s(slot + C::NODE_B, A.ulo_in + tl.node_base, nb, &full[s]);
+        bulk_g2s(slot + 2 * C::NODE_B, A.resu + tl.node_base, nb, &full[s]);
+        bulk_g2s(slot + 3 * C::NODE_B, A.geo + tl.elem_slot * kMixedGeoWords, gb, &full[s]);
+        bulk_g2s(slot + 3 * C::NODE_B + C::GEO_B, A.conn + tl.elem_slot * kMixedConnWords, cb, &full[s]);
+      }
+      if (bad) {
+        atomicExch(A.status, kStatusTimeoutCode);
+        *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
+      }
+      // drain: the newest issued fill of each slot must land before the CTA (and its smem) goes away
+      for (int s = 0; s < 2 && s < k; ++s) {
+        const int kl = s + ((k - 1 - s) >> 1) * 2;
+        mbar_wait_bounded(&full[s], (uint32_t)(kl >> 1) & 1u, kSpinLimit);
+      }
+    }
+    return;
+  }
+
+  // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h = w / 4 of its nodes
+  // and face points (8-wide chunks h, h + TPE, ...)
+  const int e = (warp & 3) * 32 + lane, h = warp >> 2;
+  const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  const float a = A.a, dt = A.dt;
+  const double b = A.b;
+  const int cons = A.conservative;
+  const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
+  const int ncodes = A.ncodes;
+  const uint32_t idv = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
+  const uint32_t idl = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NL >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
+  bool failed = false;
+  bool pend_v = false, pend_l = false;  // (thread 0) MMA groups committed and not yet seen complete
+  int k = 0;
+  for (;; ++k) {
+    const int t = blockIdx.x + k * G;
+    if (t >= A.ntiles) break;
+    const int s = k & 1;
+    const MTile tl = A.tiles[t];
+    const int ne = tl.nelem;
+    const bool valid = e < ne;
+    const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
+    float *sHi = reinterpret_cast<float *>(ring + (size_t)s * C::SLOT_B);
+    float *sLo = sHi + TE * NP;
+    float *sRe = sLo + TE * NP;
+    const float *sGeo = sRe + TE * NP;
+    const int *sCon = reinterpret_cast<const int *>(sGeo + TE * kMixedGeoWords);
+    const int ee = valid ? e : 0;
+    const float *hi = sHi + ee * NP;
+    const float *lo = sLo + ee * NP;
+    const float cr = sGeo[ee * kMixedGeoWords], cs = sGeo[ee * kMixedGeoWords + 1], ct = sGeo[ee * kMixedGeoWords + 2];
+    const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
+
+    // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into three BF16 parts ----
+    const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
+    const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
+    const double wA = cons ? 0.5 * uA * uA : uA;
+    const double dB = (cons ? 0.5 * uB * uB : uB) - wA;
+    const double dC = (cons ? 0.5 * uC * uC : uC) - wA;
+    const double dD = (cons ? 0.5 * uD * uD : uD) - wA;
+    const float L0 = (float)(0.5 * ((double)cr * dB + (double)cs * dC + (double)ct * dD));
+    if (got && valid) {
+#pragma unroll
+      for (int c = h; c < KV / 8; c += TPE) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int j = 8 * c + q;
+          v[q] = 0.f;
+          if (j < NP) {
+            const double uj = (double)hi[j] + (double)lo[j];
+            const double wj = cons ? 0.5 * uj * uj : uj;
+            v[q] = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
+          }
+        }
+        store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, v);
+      }
+    }
+    fence_async_smem();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    failed = consumers_any<CW>(!got || vload(&sMisc[0]));
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (failed) break;
+    if (tid == 0) {
+      split_gemm(tmem, saddr(sA), C::A_PART, saddr(sBV), C::BV_PART, KV, NV, idv);
+      tc_commit(mvol);
+      pend_v = true;
+    }
+
+    // ---- neighbour traces and the Lax-Friedrichs flux for this thread's face points (registers) ----
+    constexpr int NCL = (KL / 8 + TPE - 1) / TPE;  // flux chunks per thread
+    float fl[NCL][8];
+    bool bad = false;
+    const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
+#pragma unroll
+    for (int cc = 0; cc < NCL; ++cc) {
+      const int c = h + TPE * cc;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int m = 8 * c + q;
+        float v = 0.f;
+        if (c < KL / 8 && m < NF) {
+          const int f = m / NFP, p = m - f * NFP;
+          const int64_t nb = sCon[ee * kMixedConnWords + f];
+          const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
+          const int64_t idx = nb + sFt[cd * NFP + p];
+          const bool ins = (uint64_t)(idx - slot0) < (uint64_t)slotn;
+          const bool okg = (uint64_t)idx < (uint64_t)A.n_u_values;
+          bad |= valid && !ins && !okg;
+          const float uM = hi[sFm[m]];
+          const float *src = ins ? sHi + (idx - slot0) : (okg ? A.uhi_in + idx : hi + sFm[m]);
+          const float uP = *src;
+          const float g = sGeo[ee * kMixedGeoWords + 3 + f], ga = fabsf(g);
+          const float d = uM - uP;
+          v = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
+        }
+        fl[cc][q] = v;
+      }
+    }
+    if (bad) atomicExch(A.status, kStatusBadGather);
+
+    // the volume MMAs have read the A buffer (and written acc_V) once mvol completes
+    const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
+    if (vdone) pend_v = false;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (vdone && valid) {
+#pragma unroll
+      for (int cc = 0; cc < NCL; ++cc) {
+        const int c = h + TPE * cc;
+        if (c < KL / 8) store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, fl[cc]);
+      }
+    }
+    fence_async_smem();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    failed = consumers_any<CW>(!vdone);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (failed) break;
+    if (tid == 0) {
+      split_gemm(tmem + NV, saddr(sA), C::A_PART, saddr(sBL), C::BL_PART, KL, NL, idl);
+      tc_commit(mlift);
+      pend_l = true;
+    }
+
+    // ---- epilogue: both accumulators from TMEM, the stage update in FP64, the slot written back ----
+    const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
+    if (ldone) pend_l = false;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
+    if (ldone) {
+#pragma unroll 1
+      for (int c = h; c < (NP + 7) / 8; c += TPE) {
+        float dv[32];  // columns 3i+d of nodes 8c..8c+7, then their LIFT columns
+        tmem_ld8x4(lane_tmem + 24 * c, lane_tmem + 24 * c + 8, lane_tmem + 24 * c + 16, lane_tmem + NV + 8 * c, dv);
+        const float *lf = dv + 24;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int i = 8 * c + q;
+          if (i < NP && valid) {
+            const float dd = fmaf(cr, dv[3 * q], fmaf(cs, dv[3 * q + 1], fmaf(ct, dv[3 * q + 2], L0)));
+            const int o = e * NP + i;
+            const float vol = cons ? -dd : -hi[i] * dd;
+            const float t0 = fmaf(a, sRe[o], dt * vol);
+            const float rn = fmaf(dt, lf[q], t0);
+            const double un = ((double)hi[i] + (double)lo[i]) + b * (double)rn;
+            const float hn = __double2float_rn(un);
+            const float ln = __double2float_rn(un - (double)hn);
+            sHi[o] = hn;
+            sLo[o] = ln;
+            sRe[o] = rn;
+            if ((uint32_t)o >= tail0) {
+              A.uhi_out[slot0 + o] = hn;
+              A.ulo_out[slot0 + o] = ln;
+              A.resu[slot0 + o] = rn;
+            }
+          }
+        }
+      }
+    }
+    fence_async_smem();  // the slot writes become visible to the bulk stores
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    failed = consumers_any<CW>(!ldone);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (failed) break;
+    if (tid == 0) {
+      const uint32_t nbd = tail0 * 4;
+      if (nbd) {
+        bulk_s2g(A.uhi_out + slot0, sHi, nbd);
+        bulk_s2g(A.ulo_out + slot0, sLo, nbd);
+        bulk_s2g(A.resu + slot0, sRe, nbd);
+      }
+      bulk_commit();
+      bulk_wait_read_all();  // the slot may be refilled once the stores have read it
+      mbar_arrive(&empty[s]);
+    }
+  }
+  if (failed && tid == 0) {
+    atomicExch(A.status, kStatusTimeoutCode);
+    *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
+    // MMAs committed for tile k must complete before TMEM is freed (each wait is bounded)
+    if (pend_v) mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
+    if (pend_l) mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  asm volatile("bar.sync 1, %0;" ::"n"(32 * CW) : "memory");
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmCols));
+}
+
+namespace {
+
+template <int N, int CW>
+void tcm_attr() {
+  static bool done[64] = {};
+  int dev = 0;
+  cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev >= 0 && dev < 64 && done[dev]) return;
+  cuda_check(cudaFuncSetAttribute(rhs_stage_tcm_kernel<N, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+             "tcm kernel smem attribute");
+  if (dev >= 0 && dev < 64) done[dev] = true;
+}
+
+template <int N, int CW>
+bool launch_tcm_n(const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info) {
+  const uint32_t smem = tm_smem<N>(A.ncodes);
+  if (smem > 227u * 1024u) return false;
+  tcm_attr<N, CW>();
+  const int grid = std::max(1, std::min(num_sms, A.ntiles));
+  rhs_stage_tcm_kernel<N, CW><<<grid, 32 * (CW + 1), smem, st>>>(A);
+  cuda_check(cudaGetLastError(), "rhs_stage_tcm_kernel launch");
+  if (info) *info = LaunchInfo{grid, 32 * (CW + 1), (int)smem, 1};
+  return true;
+}
+
+template <int N>
+void prepare_tcm_cw(int cw) {
+  if (cw == 16)
+    tcm_attr<N, 16>();
+  else
+    tcm_attr<N, 8>();
+}
+
+template <int N>
+bool launch_tcm_cw(const MixedArgs &A, int cw, int num_sms, cudaStream_t st, LaunchInfo *info) {
+  return cw == 16 ? launch_tcm_n<N, 16>(A, num_sms, st, info) : launch_tcm_n<N, 8>(A, num_sms, st, info);
+}
+
+template <int N>
+void tcm_pack_n(const double *Dr, const double *Ds, const double *Dt, const double *LIFT, std::vector<uint16_t> &out) {
+  using C = TmCfg<N>;
+  constexpr int NP = C::NP, NF = C::NF, KV = C::KV, KL = C::KL, NV = C::NV, NL = C::NL;
+  out.assign(C::CONST_BYTES / 2, 0);
+  auto put = [&](size_t base, size_t part, int R, int r, int k, double x) {
+    double rem = x;
+    for (int p = 0; p < 3; ++p) {
+      const __nv_bfloat16 v = __float2bfloat16_rn((float)rem);
+      out[base + p * part + (size_t)kmaj(r, k, R)] = *reinterpret_cast<const uint16_t *>(&v);
+      rem -= (double)__bfloat162float(v);
+    }
+  };
+  const double *D[3] = {Dr, Ds, Dt};
+  const size_t pv = (size_t)NV * KV, pl = (size_t)NL * KL;
+  for (int i = 0; i < NP; ++i)
+    for (int d = 0; d < 3; ++d)
+      for (int j = 0; j < NP; ++j) put(0, pv, NV, 3 * i + d, j, D[d][i * NP + j]);
+  for (int i = 0; i < NP; ++i)
+    for (int m = 0; m < NF; ++m) put(3 * pv, pl, NL, i, m, LIFT[(size_t)i * NF + m]);
+}
+
+}  // namespace
+
+int tcm_tile_elems() { return kTmTE; }
+
+bool tcm_supported(int N) { return N >= 1 && N <= 4; }
+
+void tcm_pack_operands(int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
+                       std::vector<uint16_t> &out) {
+  switch (N) {
+    case 1: tcm_pack_n<1>(Dr, Ds, Dt, LIFT, out); break;
+    case 2: tcm_pack_n<2>(Dr, Ds, Dt, LIFT, out); break;
+    case 3: tcm_pack_n<3>(Dr, Ds, Dt, LIFT, out); break;
+    case 4: tcm_pack_n<4>(Dr, Ds, Dt, LIFT, out); break;
+    default: out.clear();
+  }
+}
+
+void prepare_rhs_tcm(int N, int consumer_warps) {
+  switch (N) {
+    case 1: prepare_tcm_cw<1>(consumer_warps); break;
+    case 2: prepare_tcm_cw<2>(consumer_warps); break;
+    case 3: prepare_tcm_cw<3>(consumer_warps); break;
+    case 4: prepare_tcm_cw<4>(consumer_warps); break;
+    default: break;
+  }
+}
+
+bool launch_rhs_tcm(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st, LaunchInfo *info) {
+  switch (N) {
+    case 1: return launch_tcm_cw<1>(A, consumer_warps, num_sms, st, info);
+    case 2: return launch_tcm_cw<2>(A, consumer_warps, num_sms, st, info);
+    case 3: return launch_tcm_cw<3>(A, consumer_warps, num_sms, st, info);
+    case 4: return launch_tcm_cw<4>(A, consumer_warps, num_sms, st, info);
+    default: return false;
+  }
+}
+
+}  // namespace dgk

@@ -1,0 +1,65 @@
+"""Parity of the tensor-core mixed stage (rhsStageMixed with mma=1: the element-local products as GEMMs on
+tcgen05 with three-part BF16 operands and FP32 accumulation) with the FP64 oracle, through the runner / C ABI.
+
+Bounds, relative L2 against the oracle's FP64 state after 10 LSERK4 stages of smooth random-mode fields:
+MMA_TOL = 1e-7, the bound of the FP32-product mixed stage (the three-part split keeps about 24 significant
+bits of every operand; measured 3.5e-8 .. 6.7e-8); the same for the conservative form, for both launch shapes
+(2 and 4 threads per element) and for partitions whose element counts are not multiples of the 128-element
+tile (partial tiles, and slot copies that end inside a 16-byte word).
+"""
+import numpy as np
+import pytest
+
+from dgkernel_b200.burgers import BurgersProblem, MIXED
+from oracle import burgers_ref as b
+from oracle import oracle as O
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+MMA_TOL = 1e-7
+
+
+def _oracle_run(N, n, nslab, u0, dt, nstages, conservative=0):
+    ref = b.Problem(N, n, nslab, "sine")
+    rs = O.RunState(ref)
+    u = np.ascontiguousarray(u0, dtype=np.float64).copy()
+    resu = np.zeros_like(u)
+    rs.run(u, resu, dt, nstages, conservative=conservative, threads=4)
+    return u
+
+
+@pytest.mark.parametrize("N,n,nslab,warps", [(4, 4, 2, 16), (4, 4, 2, 8), (3, 5, 5, 16), (2, 6, 3, 16),
+                                             (1, 6, 2, 8), (4, 7, 7, 16)])
+def test_tcm_stage_matches_fp64_oracle(N, n, nslab, warps):
+    P = BurgersProblem(N, n, nslab, MIXED, "modes", mma=True, warps=warps)
+    u0 = P.u0.copy()
+    P.run_stages(10)
+    got = P.get("u")
+    want = _oracle_run(N, n, nslab, u0, P.dt, 10)
+    err = rel_l2(got, want)
+    print(f"order {N} n {n} warps {warps}: relative L2 {err:.3e}")
+    assert err < MMA_TOL, err
+    P.free()
+
+
+def test_tcm_stage_conservative_form():
+    P = BurgersProblem(4, 5, 5, MIXED, "modes", conservative=1, mma=True)
+    u0 = P.u0.copy()
+    P.run_stages(10)
+    want = _oracle_run(4, 5, 5, u0, P.dt, 10, conservative=1)
+    assert rel_l2(P.get("u"), want) < MMA_TOL
+    P.free()
+
+
+def test_tcm_stage_tracks_simt_mixed_stage():
+    """Many tiles per CTA (16^3 x 6 = 24,576 elements, 192 tiles): the tensor-core and FP32-FMA forms of the
+    same stage stay within the mixed bound of each other over 25 stages."""
+    A = BurgersProblem(4, 16, 4, MIXED, "modes")
+    B = BurgersProblem(4, 16, 4, MIXED, "modes", mma=True)
+    A.run_stages(25)
+    B.run_stages(25)
+    assert np.isfinite(B.get("u")).all()
+    assert rel_l2(B.get("u"), A.get("u")) < MMA_TOL
+    A.free()
+    B.free()
