@@ -1,11 +1,12 @@
 """Benchmark of the tet-DG RHS hot path on B200: DOF-stage-updates/s of LSERK4 stages.
 
-Workload: 3-D scalar Burgers, nodal DG order N=4 (Np=35, Nfp=15) on a periodic 64^3 x 6
+Default workload: 3-D scalar Burgers, nodal DG order N=4 (Np=35, Nfp=15) on a periodic 64^3 x 6
 Kuhn-cube mesh (K = 1,572,864 tets), 16 x-slab partitions, u0 = 0.5 + 8 seeded random Fourier modes.  One
 "step" is one LSERK4 stage over all K elements: the fused volume + Lax-Friedrichs surface + LIFT + stage update
-kernel.  Three forms run from the same initial state: plain FP64 (rhsStage, reference-contract layout), plain
-FP32, and mixed (rhsStageMixed: compensated FP32 state, FP32 products on the element's higher-order part,
-compact affine geometry and compressed face maps).  `value` is the chosen form: the fastest one whose
+kernel.  Four forms run from the same initial state: plain FP64 (rhsStage, reference-contract layout), plain
+FP32, mixed (rhsStageMixed: compensated FP32 state, FP32 products on the element's higher-order part,
+compact affine geometry and compressed face maps) and mixed_tc (the same stage with its products on the tensor
+cores, three-part BF16 operands, FP32 accumulation).  `value` is the chosen form: the fastest one whose
 relative L2 error against the FP64 run stays <= 1e-6 at t_final (after the warm-up and timed stages).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 64] [--order 4]
@@ -192,7 +193,7 @@ def run_reference(args, world, rank):
 
 
 def run_ensemble(args, world, rank, local):
-    """Config 4: 256 independent order-3 instances, n_i ~ U{6..24} (seeded), FP32 compensated state (mixed
+    """Batching workload: 256 independent order-3 instances, n_i ~ U{6..24} (seeded), FP32 compensated state (mixed
     stage), one persistent launch per stage, stages replayed from a captured CUDA graph, autotuned shape."""
     import torch
     from dgkernel_b200.burgers import BurgersEnsemble, ensemble_sizes
@@ -219,7 +220,7 @@ def run_ensemble(args, world, rank, local):
     ms = max_over_ranks(e0.elapsed_time(e1) / (10 * reps), world)
     ok = bool(np.isfinite(E.get("u")).all())
     if rank == 0:
-        out = {"metric": "DOF-stage-updates/s, batching form (config 4)", "value": world * E.dofs / (ms * 1e-3),
+        out = {"metric": "DOF-stage-updates/s, batching form (256 order-3 instances)", "value": world * E.dofs / (ms * 1e-3),
                "unit": UNIT, "n_gpus": world, "steps": 10 * reps, "warmup": 10, "ms_per_step": ms,
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32x2+f32",
                "data": "synthetic",
@@ -235,7 +236,7 @@ def run_ensemble(args, world, rank, local):
 
 
 def run_precision(args, world, rank, local):
-    """Config 3: order 7, 32^3 x 6 Kuhn mesh, u0 = 0.5 + 0.25 sin(pi x) cos(pi y) sin(pi z), to t = 0.2: the
+    """Precision workload: order 7, 32^3 x 6 Kuhn mesh, u0 = 0.5 + 0.25 sin(pi x) cos(pi y) sin(pi z), to t = 0.2: the
     precision form (tcgen05 BF16 hi/lo GEMMs, FP32 accumulation, compensated FP32 state) against the FP64 run.
     The same run at order 4 is reported beside it: on the reference's order-7 node set the split products lose
     every digit of the derivative and the run leaves the stable range."""
@@ -273,7 +274,7 @@ def run_precision(args, world, rank, local):
             "clocks": res["tc"]["clk"]}
     if rank == 0:
         m = per_order[7]
-        out = {"metric": "DOF-stage-updates/s, precision form (config 3)", "value": m["tc_value"], "unit": UNIT,
+        out = {"metric": "DOF-stage-updates/s, precision form (order 7, 32^3x6)", "value": m["tc_value"], "unit": UNIT,
                "n_gpus": world, "steps": m["stages"], "warmup": args.warmup, "ms_per_step": m["tc_ms_per_step"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3 (fp32 acc)",
                "data": "synthetic",
@@ -286,7 +287,7 @@ def run_precision(args, world, rank, local):
 
 
 def run_learned(args, world, rank, local):
-    """Config 5: shock-forming u0 = 0.5 + sin sin sin, order 4, 48^3 x 6, to t = 0.5 with artificial viscosity.
+    """Learned-sensor workload: shock-forming u0 = 0.5 + sin sin sin, order 4, 48^3 x 6, to t = 0.5 with artificial viscosity.
     The sensor network is trained first (library kernels) on (modal features, PP activation) pairs from PP
     runs on random-mode fields; then the PP-sensor FP64 solution (the judge) and the learned-sensor solution
     run to t_final.  Reports both stage rates and the relative L1 error of the learned run."""
@@ -340,7 +341,7 @@ def run_learned(args, world, rank, local):
     l1 = float(np.abs(runs["mlp"]["u"] - ref).sum() / np.abs(ref).sum()) if all(finite.values()) else None
     if rank == 0:
         m = runs["mlp"]
-        out = {"metric": "DOF-stage-updates/s, learned-sensor form (config 5)", "value": world * m["dofs"] / (m["ms"] * 1e-3),
+        out = {"metric": "DOF-stage-updates/s, learned-sensor form (order 4, 48^3x6 shock)", "value": world * m["dofs"] / (m["ms"] * 1e-3),
                "unit": UNIT, "n_gpus": world, "steps": m["stages"], "warmup": args.warmup, "ms_per_step": m["ms"],
                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 (sensor f16/f32)",
                "data": "synthetic",
@@ -366,7 +367,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="burgers", choices=["burgers", "ensemble", "learned", "precision"],
-                    help="burgers: config 2 (default); precision: config 3; ensemble: config 4; learned: config 5")
+                    help="burgers: order 4, 64^3x6 (default); precision: order 7, 32^3x6; ensemble: 256 order-3 "
+                         "instances; learned: order 4, 48^3x6 shock with the learned sensor")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup(args)
@@ -387,7 +389,8 @@ def main():
 
 
 def run_burgers(args, world, rank, local):
-    """Config 2 (the default line): plain FP64, plain FP32 and mixed forms from one u0; the chosen form."""
+    """The default line (order 4, 64^3 x 6): plain FP64, plain FP32 and the mixed forms from one u0; the chosen
+    form."""
     import torch
     from dgkernel_b200.burgers import BurgersProblem, RK4A, RK4B, MIXED
     torch.cuda.set_device(local)
@@ -395,9 +398,14 @@ def run_burgers(args, world, rank, local):
     hbm, peak_kind = peaks()
     results = {}
     finals = {}
-    forms = (("f64", np.float64), ("f32", np.float32), ("mixed", MIXED))
-    for name, dt in forms:
-        prob = BurgersProblem(args.order, args.n, args.slabs, dt, "modes", stream=stream.cuda_stream)
+    # mixed_tc: the mixed stage with its element-local products on the tensor cores (orders 1..4)
+    forms = [("f64", np.float64, {}), ("f32", np.float32, {}), ("mixed", MIXED, {})]
+    if args.order <= 4:
+        forms.append(("mixed_tc", MIXED, {"mma": True}))
+    kernels = {"f64": "rhs_stage_dmma_kernel", "f32": "rhs_stage_kernel", "mixed": "rhs_stage_mixed_kernel",
+               "mixed_tc": "rhs_stage_tcm_kernel"}
+    for name, dt, kw in forms:
+        prob = BurgersProblem(args.order, args.n, args.slabs, dt, "modes", stream=stream.cuda_stream, **kw)
         prob.run_stages(args.warmup)
         barrier(world)
         with ClockSampler(local) as clk:
@@ -405,10 +413,9 @@ def run_burgers(args, world, rank, local):
         ms = max_over_ranks(ms, world)
         finals[name] = prob.get("u").astype(np.float64)
         results[name] = {"ms": ms, "dofs": prob.dofs, "clocks": clk.summary(), "prob": prob,
-                         "b_alg": b_alg_mixed(args.order) if name == "mixed" else
+                         "b_alg": b_alg_mixed(args.order) if name.startswith("mixed") else
                          b_alg_per_dof(args.order, 8 if name == "f64" else 4),
-                         "kernel": "rhs_stage_mixed_kernel" if name == "mixed" else
-                         ("rhs_stage_dmma_kernel" if name == "f64" else "rhs_stage_kernel")}
+                         "kernel": kernels[name]}
         if name != "f64":
             prob.free()
     ref = finals["f64"]
@@ -424,10 +431,11 @@ def run_burgers(args, world, rank, local):
     prob = results["f64"]["prob"]
     if chosen != "f64":
         prob.free()
-        prob = BurgersProblem(args.order, args.n, args.slabs, MIXED if chosen == "mixed" else np.float32, "modes",
-                              stream=stream.cuda_stream)
+        dt_kw = {k: (d, kw) for k, d, kw in forms}[chosen]
+        prob = BurgersProblem(args.order, args.n, args.slabs, dt_kw[0], "modes", stream=stream.cuda_stream,
+                              **dt_kw[1])
     r = prob.runner
-    state = ("uhi", "ulo", "resu") if chosen == "mixed" else ("u", "resu")
+    state = ("uhi", "ulo", "resu") if chosen.startswith("mixed") else ("u", "resu")
     hdt = torch.float32 if chosen != "f64" else torch.float64
     hosts = {nm: torch.empty(dofs, dtype=hdt, pin_memory=True).numpy() for nm in state}
     for nm, h in hosts.items():
@@ -436,7 +444,7 @@ def run_burgers(args, world, rank, local):
     kc = r.KernelConfigs["rhsStage"]
     params = [r.Param(p.name).Copy() if p.name in state else r.Param(p.name) for p in kc.params]
     r.ConfigureKernel("stageE2E", *params)
-    r.BuildKernel(("rhsStageMixed" if chosen == "mixed" else "rhsStage"), "stageE2E")
+    r.BuildKernel(prob.op_id(), "stageE2E")
     r.ExecuteKernel("stageE2E", RK4A[0], RK4B[0], prob.dt)
     barrier(world)
     torch.cuda.synchronize()
@@ -469,7 +477,8 @@ def run_burgers(args, world, rank, local):
         out = {
             "metric": METRIC, "value": thr[chosen], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ch["ms"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "mixed": "f32x2+f32"}[chosen],
+            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "mixed": "f32x2+f32",
+                                                  "mixed_tc": "f32x2+f32 (bf16x3 products, f32 acc)"}[chosen],
             "data": "synthetic",
             "config": {"workload": f"3-D Burgers tet-DG, order {args.order} (Np={Np}), periodic {args.n}^3x6 Kuhn "
                                    f"mesh (K={dofs // Np}), {args.slabs} x-slab partitions, u0 = 0.5 + 8 seeded "

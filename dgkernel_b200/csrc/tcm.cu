@@ -69,27 +69,24 @@ __host__ __device__ constexpr uint32_t tm_smem(int ncodes) {
   return TmCfg<N>::OFF_FTAB + (((uint32_t)ncodes * TmCfg<N>::NFP + 15u) & ~15u);
 }
 
-__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
-  return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(a)) |
-         ((uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(b)) << 16);
+// Round a pair to BF16 (one paired conversion): the packed bits, low half = x, and the residuals x - bf16(x).
+__device__ __forceinline__ uint32_t bf16_pair(float &x, float &y) {
+  const __nv_bfloat162 p = __float22bfloat162_rn(make_float2(x, y));
+  const uint32_t w = *reinterpret_cast<const uint32_t *>(&p);
+  x -= __uint_as_float(w << 16);
+  y -= __uint_as_float(w & 0xffff0000u);
+  return w;
 }
 
 // Split 8 values into three BF16 parts and store each part's 16 bytes at `dst + p * part_bytes`.
 __device__ __forceinline__ void store_split8(unsigned char *dst, uint32_t part_bytes, const float (&v)[8]) {
-  float r1[8], r2[8];
   uint32_t w0[4], w1[4], w2[4];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    const float x0 = __bfloat162float(__float2bfloat16_rn(v[q]));
-    r1[q] = v[q] - x0;
-    const float x1 = __bfloat162float(__float2bfloat16_rn(r1[q]));
-    r2[q] = r1[q] - x1;
-  }
-#pragma unroll
   for (int q = 0; q < 4; ++q) {
-    w0[q] = pack_bf16(v[2 * q], v[2 * q + 1]);
-    w1[q] = pack_bf16(r1[2 * q], r1[2 * q + 1]);
-    w2[q] = pack_bf16(r2[2 * q], r2[2 * q + 1]);
+    float x = v[2 * q], y = v[2 * q + 1];  // residuals are exact in FP32
+    w0[q] = bf16_pair(x, y);
+    w1[q] = bf16_pair(x, y);
+    w2[q] = bf16_pair(x, y);
   }
   *reinterpret_cast<uint4 *>(dst) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
   *reinterpret_cast<uint4 *>(dst + part_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
@@ -108,23 +105,21 @@ __device__ __forceinline__ bool consumers_any(bool v) {
   return r != 0;
 }
 
-// Four 8-column TMEM loads of this warp's lanes under one wait.
-__device__ __forceinline__ void tmem_ld8x4(uint32_t t0, uint32_t t1, uint32_t t2, uint32_t t3, float (&v)[32]) {
-  uint32_t r[32];
+// 24 consecutive TMEM columns (three 8-column loads) of this warp's lanes under one wait.
+__device__ __forceinline__ void tmem_ld24(uint32_t t0, float (&v)[24]) {
+  uint32_t r[24];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%32];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%33];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16,%17,%18,%19,%20,%21,%22,%23}, [%34];\n\t"
-      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%24,%25,%26,%27,%28,%29,%30,%31}, [%35];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%24];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%8,%9,%10,%11,%12,%13,%14,%15}, [%25];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%16,%17,%18,%19,%20,%21,%22,%23}, [%26];\n\t"
       "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(t0), "r"(t1), "r"(t2), "r"(t3)
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23])
+      : "r"(t0), "r"(t0 + 8), "r"(t0 + 16)
       : "memory");
 #pragma unroll
-  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+  for (int j = 0; j < 24; ++j) v[j] = __uint_as_float(r[j]);
 }
 
 // One GEMM of the split products: 6 MMAs per 16-wide K step into the accumulator at `acc`.
@@ -230,9 +225,10 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     return;
   }
 
-  // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h = w / 4 of its nodes
-  // and face points (8-wide chunks h, h + TPE, ...)
-  const int e = (warp & 3) * 32 + lane, h = warp >> 2;
+  // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h of its nodes and face
+  // points (8-wide chunks h, h + TPE, ...), h = TPE - 1 - w / 4 so that the warps of thread 0 (which issues the
+  // MMAs) take the shares with fewer chunks
+  const int e = (warp & 3) * 32 + lane, h = TPE - 1 - (warp >> 2);
   const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const float a = A.a, dt = A.dt;
   const double b = A.b;
@@ -262,6 +258,36 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     const float *lo = sLo + ee * NP;
     const float cr = sGeo[ee * kMixedGeoWords], cs = sGeo[ee * kMixedGeoWords + 1], ct = sGeo[ee * kMixedGeoWords + 2];
     const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
+
+    // ---- neighbour traces for this thread's face points, loaded first so that their latency overlaps dw ----
+    constexpr int NCL = (KL / 8 + TPE - 1) / TPE;  // flux chunks per thread
+    float fl[NCL][8];                               // uP, then the flux
+    {
+      bool bad = false;
+      const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
+#pragma unroll
+      for (int cc = 0; cc < NCL; ++cc) {
+        const int c = h + TPE * cc;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int m = 8 * c + q;
+          float v = 0.f;
+          if (got && c < KL / 8 && m < NF) {
+            const int f = m / NFP, p = m - f * NFP;
+            const int64_t nb = sCon[ee * kMixedConnWords + f];
+            const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
+            const int64_t idx = nb + sFt[cd * NFP + p];
+            const bool ins = (uint64_t)(idx - slot0) < (uint64_t)slotn;
+            const bool okg = (uint64_t)idx < (uint64_t)A.n_u_values;
+            bad |= valid && !ins && !okg;
+            const float *src = ins ? sHi + (idx - slot0) : (okg ? A.uhi_in + idx : hi + sFm[m]);
+            v = *src;
+          }
+          fl[cc][q] = v;
+        }
+      }
+      if (bad) atomicExch(A.status, kStatusBadGather);
+    }
 
     // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into three BF16 parts ----
     const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
@@ -299,37 +325,22 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
       pend_v = true;
     }
 
-    // ---- neighbour traces and the Lax-Friedrichs flux for this thread's face points (registers) ----
-    constexpr int NCL = (KL / 8 + TPE - 1) / TPE;  // flux chunks per thread
-    float fl[NCL][8];
-    bool bad = false;
-    const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
+    // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
 #pragma unroll
     for (int cc = 0; cc < NCL; ++cc) {
       const int c = h + TPE * cc;
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int m = 8 * c + q;
-        float v = 0.f;
         if (c < KL / 8 && m < NF) {
-          const int f = m / NFP, p = m - f * NFP;
-          const int64_t nb = sCon[ee * kMixedConnWords + f];
-          const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
-          const int64_t idx = nb + sFt[cd * NFP + p];
-          const bool ins = (uint64_t)(idx - slot0) < (uint64_t)slotn;
-          const bool okg = (uint64_t)idx < (uint64_t)A.n_u_values;
-          bad |= valid && !ins && !okg;
-          const float uM = hi[sFm[m]];
-          const float *src = ins ? sHi + (idx - slot0) : (okg ? A.uhi_in + idx : hi + sFm[m]);
-          const float uP = *src;
+          const int f = m / NFP;
+          const float uM = hi[sFm[m]], uP = fl[cc][q];
           const float g = sGeo[ee * kMixedGeoWords + 3 + f], ga = fabsf(g);
           const float d = uM - uP;
-          v = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
+          fl[cc][q] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
         }
-        fl[cc][q] = v;
       }
     }
-    if (bad) atomicExch(A.status, kStatusBadGather);
 
     // the volume MMAs have read the A buffer (and written acc_V) once mvol completes
     const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
@@ -353,36 +364,54 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
       pend_l = true;
     }
 
-    // ---- epilogue: both accumulators from TMEM, the stage update in FP64, the slot written back ----
+    // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
+    constexpr int NCE = ((NP + 7) / 8 + TPE - 1) / TPE;  // epilogue chunks per thread
+    float t0[NCE][8];
+#pragma unroll
+    for (int cc = 0; cc < NCE; ++cc) {
+      const int c = h + TPE * cc;
+      if (c < (NP + 7) / 8) {
+        float dv[24];  // columns 3i+d of nodes 8c..8c+7
+        tmem_ld24(lane_tmem + 24 * c, dv);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int i = min(8 * c + q, NP - 1);
+          const float dd = fmaf(cr, dv[3 * q], fmaf(cs, dv[3 * q + 1], fmaf(ct, dv[3 * q + 2], L0)));
+          const float vol = cons ? -dd : -hi[i] * dd;
+          t0[cc][q] = fmaf(a, sRe[ee * NP + i], dt * vol);
+        }
+      }
+    }
+
+    // ---- LIFT accumulator, the stage update in FP64, the slot written back ----
     const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
     if (ldone) pend_l = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
     if (ldone) {
-#pragma unroll 1
-      for (int c = h; c < (NP + 7) / 8; c += TPE) {
-        float dv[32];  // columns 3i+d of nodes 8c..8c+7, then their LIFT columns
-        tmem_ld8x4(lane_tmem + 24 * c, lane_tmem + 24 * c + 8, lane_tmem + 24 * c + 16, lane_tmem + NV + 8 * c, dv);
-        const float *lf = dv + 24;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int i = 8 * c + q;
-          if (i < NP && valid) {
-            const float dd = fmaf(cr, dv[3 * q], fmaf(cs, dv[3 * q + 1], fmaf(ct, dv[3 * q + 2], L0)));
-            const int o = e * NP + i;
-            const float vol = cons ? -dd : -hi[i] * dd;
-            const float t0 = fmaf(a, sRe[o], dt * vol);
-            const float rn = fmaf(dt, lf[q], t0);
-            const double un = ((double)hi[i] + (double)lo[i]) + b * (double)rn;
-            const float hn = __double2float_rn(un);
-            const float ln = __double2float_rn(un - (double)hn);
-            sHi[o] = hn;
-            sLo[o] = ln;
-            sRe[o] = rn;
-            if ((uint32_t)o >= tail0) {
-              A.uhi_out[slot0 + o] = hn;
-              A.ulo_out[slot0 + o] = ln;
-              A.resu[slot0 + o] = rn;
+      for (int cc = 0; cc < NCE; ++cc) {
+        const int c = h + TPE * cc;
+        if (c < (NP + 7) / 8) {
+          float lf[8];
+          tmem_ld8(lane_tmem + NV + 8 * c, lf);
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const int i = 8 * c + q;
+            if (i < NP && valid) {
+              const int o = e * NP + i;
+              const float rn = fmaf(dt, lf[q], t0[cc][q]);
+              const double un = ((double)hi[i] + (double)lo[i]) + b * (double)rn;
+              const float hn = __double2float_rn(un);
+              const float ln = __double2float_rn(un - (double)hn);
+              sHi[o] = hn;
+              sLo[o] = ln;
+              sRe[o] = rn;
+              if ((uint32_t)o >= tail0) {
+                A.uhi_out[slot0 + o] = hn;
+                A.ulo_out[slot0 + o] = ln;
+                A.resu[slot0 + o] = rn;
+              }
             }
           }
         }

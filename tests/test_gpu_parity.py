@@ -135,7 +135,7 @@ def test_rhs_lf_fp32(c1):
 
 
 def test_stage_trajectory_c1_fp64(c1):
-    # 10 LSERK4 steps (50 stages, t = 0.75) of config 1, before the unlimited solution blows up past the shock
+    # 10 LSERK4 steps (50 stages, t = 0.75) of the order-2 8^3 x 6 sine case, before the unlimited solution blows up past the shock
     P = BurgersProblem(2, 8, 4, np.float64, "sine")
     u = np.ascontiguousarray(c1.u0.reshape(-1)).copy()
     resu = np.zeros_like(u)
@@ -259,7 +259,7 @@ def test_bad_gather_index_is_reported_not_faulted(c1):
 
 
 def test_full_size_conservation_and_fp32_tracking():
-    # config 2 size (N=4, 64^3 x 6 = 1,572,864 tets, 16 slabs): the conservative strong form conserves the
+    # full benchmark size (N=4, 64^3 x 6 = 1,572,864 tets, 16 slabs): the conservative strong form conserves the
     # integral of u exactly on the periodic mesh; the FP32 run tracks the FP64 run
     el = d.Element(4)
     w = el.MassMatrix.sum(axis=0)  # integral weights of the reference element (J is constant per tet)
