@@ -20,8 +20,8 @@
 // threads write the split dw into the A buffer (K-major canonical layout), one thread issues the volume MMAs,
 // the threads gather the neighbour traces and form the flux meanwhile, write it into the same A buffer once
 // the volume MMAs have completed, one thread issues the LIFT MMAs, and the threads read both accumulators from
-// TMEM, finish the stage in FP64 and write the slot back with bulk stores.  Constant operands (D and LIFT,
-// split) stay in shared memory for the whole launch.  Every wait is bounded; a failed wait sets the status
+// TMEM and finish the stage in FP64 into the slot, which the producer writes back with bulk stores before it
+// refills it.  Constant operands (D and LIFT, split) stay in shared memory for the whole launch.  Every wait is bounded; a failed wait sets the status
 // word and the CTA leaves after draining its copies and MMAs; TMEM is always freed.
 #include <cuda_bf16.h>
 
@@ -56,7 +56,7 @@ struct TmCfg {
   // shared-memory layout (bytes)
   static constexpr uint32_t OFF_BV = 0, OFF_BL = OFF_BV + 3 * BV_PART, OFF_A = OFF_BL + 3 * BL_PART;
   static constexpr uint32_t OFF_SLOT = OFF_A + 3 * A_PART, OFF_BARY = OFF_SLOT + 2 * SLOT_B;
-  static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;  // full[2], empty[2], vol, lift
+  static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;  // full[2], done[2], vol, lift
   static constexpr uint32_t OFF_MISC = OFF_BARS + 6 * 8;                  // abort flag, TMEM base
   static constexpr uint32_t OFF_FMASK = OFF_MISC + 16;
   static constexpr uint32_t OFF_FTAB = OFF_FMASK + ((NF + 15) & ~15);
@@ -141,7 +141,7 @@ __device__ __forceinline__ int vload(const int *p) { return *reinterpret_cast<co
 
 }  // namespace
 
-// CW = 8 or 16 consumer warps: CW / 4 threads per element.
+// CW = 8, 12, 16 or 20 consumer warps: CW / 4 threads per element.
 template <int N, int CW>
 __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const MixedArgs A) {
   using C = TmCfg<N>;
@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   unsigned char *sBV = sm + C::OFF_BV, *sBL = sm + C::OFF_BL, *sA = sm + C::OFF_A;
   unsigned char *ring = sm + C::OFF_SLOT;
   double *sBary = reinterpret_cast<double *>(sm + C::OFF_BARY);
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *empty = full + 2, *mvol = full + 4,
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *done = full + 2, *mvol = full + 4,
            *mlift = full + 5;
   int *sMisc = reinterpret_cast<int *>(sm + C::OFF_MISC);  // [0] abort flag, [1] TMEM base
   uint8_t *sFm = sm + C::OFF_FMASK, *sFt = sm + C::OFF_FTAB;
@@ -169,7 +169,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   for (int x = tid; x < NF; x += blockDim.x) sFm[x] = (uint8_t)A.fmask[x];
   for (int x = tid; x < A.ncodes * NFP; x += blockDim.x) sFt[x] = A.ftab[x];
   if (tid == 0) {
-    for (int b = 0; b < 6; ++b) mbar_init(&full[b], 1);
+    for (int b = 0; b < 6; ++b) mbar_init(&full[b], (b == 2 || b == 3) ? 32 * CW : 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     sMisc[0] = 0;
   }
@@ -184,23 +184,43 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = (uint32_t)sMisc[1];
 
-  if (warp == CW) {  // producer: lane 0 streams this CTA's tiles through the 2-slot ring
+  if (warp == CW) {
+    // producer, lane 0: streams this CTA's tiles through the 2-slot ring and writes each finished slot back.
+    // Slot s holds tile k, then k + 2: once every consumer thread has arrived on done[s] for tile k, the slot's
+    // hi, lo and resu go out with bulk stores (the ragged tail past the last full 16 bytes was written by the
+    // consumers), and the refill starts when the stores have read the slot.
     if (lane == 0) {
+      MTile held[2] = {};
+      auto store = [&](int s, const MTile &tl) {
+        const uint32_t nbd = (((uint32_t)(tl.nelem * NP * 4)) & ~15u);
+        unsigned char *slot = ring + (size_t)s * C::SLOT_B;
+        if (nbd) {
+          bulk_s2g(A.uhi_out + tl.node_base, slot, nbd);
+          bulk_s2g(A.ulo_out + tl.node_base, slot + C::NODE_B, nbd);
+          bulk_s2g(A.resu + tl.node_base, slot + 2 * C::NODE_B, nbd);
+        }
+        bulk_commit();
+      };
       int k = 0;
       bool bad = false;
       for (;; ++k) {
         const int t = blockIdx.x + k * G;
         if (t >= A.ntiles) break;
         const int s = k & 1;
-        if (k >= 2 && !mbar_wait_bounded(&empty[s], (uint32_t)((k >> 1) - 1) & 1u, kSpinLimit)) {
-          bad = true;
-          break;
+        if (k >= 2) {
+          if (!mbar_wait_bounded(&done[s], (uint32_t)((k - 2) >> 1) & 1u, kSpinLimit)) {
+            bad = true;
+            break;
+          }
+          store(s, held[s]);
+          bulk_wait_read_all();  // the slot may be refilled once the stores have read it
         }
         if (vload(&sMisc[0])) {
           bad = true;
           break;
         }
         const MTile tl = A.tiles[t];
+        held[s] = tl;
         unsigned char *slot = ring + (size_t)s * C::SLOT_B;
         const uint32_t nb = round16((uint32_t)(tl.nelem * NP * 4));
         const uint32_t gb = (uint32_t)tl.nelem * kMixedGeoWords * 4;
@@ -212,14 +232,26 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
         bulk_g2s(slot + 3 * C::NODE_B, A.geo + tl.elem_slot * kMixedGeoWords, gb, &full[s]);
         bulk_g2s(slot + 3 * C::NODE_B + C::GEO_B, A.conn + tl.elem_slot * kMixedConnWords, cb, &full[s]);
       }
+      if (!bad) {
+        // the last one or two tiles: write them back once their consumers are done
+        for (int j = (k >= 2 ? k - 2 : 0); j < k && !bad; ++j) {
+          if (!mbar_wait_bounded(&done[j & 1], (uint32_t)(j >> 1) & 1u, kSpinLimit)) {
+            bad = true;
+            break;
+          }
+          store(j & 1, held[j & 1]);
+        }
+        bulk_wait_read_all();
+      }
       if (bad) {
         atomicExch(A.status, kStatusTimeoutCode);
         *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
-      }
-      // drain: the newest issued fill of each slot must land before the CTA (and its smem) goes away
-      for (int s = 0; s < 2 && s < k; ++s) {
-        const int kl = s + ((k - 1 - s) >> 1) * 2;
-        mbar_wait_bounded(&full[s], (uint32_t)(kl >> 1) & 1u, kSpinLimit);
+        // drain: the newest issued fill of each slot must land before the CTA (and its smem) goes away
+        for (int s = 0; s < 2 && s < k; ++s) {
+          const int kl = s + ((k - 1 - s) >> 1) * 2;
+          mbar_wait_bounded(&full[s], (uint32_t)(kl >> 1) & 1u, kSpinLimit);
+        }
+        bulk_wait_read_all();
       }
     }
     return;
@@ -237,14 +269,20 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   const int ncodes = A.ncodes;
   const uint32_t idv = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
   const uint32_t idl = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NL >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
-  bool failed = false;
+  // gathered indices fit 32 bits (the compact connectivity stores int32 bases)
+  const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
+  bool failed = false, prev_bad = false;  // prev_bad: the previous tile's LIFT wait failed
   bool pend_v = false, pend_l = false;  // (thread 0) MMA groups committed and not yet seen complete
+  uint32_t par_v = 0, par_l = 0;         // their mbarrier phases
+  MTile tl_next{};
+  if ((int)blockIdx.x < A.ntiles) tl_next = A.tiles[blockIdx.x];
   int k = 0;
   for (;; ++k) {
     const int t = blockIdx.x + k * G;
     if (t >= A.ntiles) break;
     const int s = k & 1;
-    const MTile tl = A.tiles[t];
+    const MTile tl = tl_next;
+    if (t + G < A.ntiles) tl_next = A.tiles[t + G];  // the next descriptor's load overlaps this tile
     const int ne = tl.nelem;
     const bool valid = e < ne;
     const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
@@ -274,13 +312,14 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
           float v = 0.f;
           if (got && c < KL / 8 && m < NF) {
             const int f = m / NFP, p = m - f * NFP;
-            const int64_t nb = sCon[ee * kMixedConnWords + f];
+            const uint32_t nb = (uint32_t)sCon[ee * kMixedConnWords + f];
             const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
-            const int64_t idx = nb + sFt[cd * NFP + p];
-            const bool ins = (uint64_t)(idx - slot0) < (uint64_t)slotn;
-            const bool okg = (uint64_t)idx < (uint64_t)A.n_u_values;
+            const uint32_t idx = nb + sFt[cd * NFP + p];
+            const uint32_t loc = idx - (uint32_t)slot0;
+            const bool ins = loc < (uint32_t)slotn;
+            const bool okg = idx < n_u32;
             bad |= valid && !ins && !okg;
-            const float *src = ins ? sHi + (idx - slot0) : (okg ? A.uhi_in + idx : hi + sFm[m]);
+            const float *src = ins ? sHi + loc : (okg ? A.uhi_in + idx : hi + sFm[m]);
             v = *src;
           }
           fl[cc][q] = v;
@@ -316,13 +355,14 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     }
     fence_async_smem();
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    failed = consumers_any<CW>(!got || vload(&sMisc[0]));
+    failed = consumers_any<CW>(!got || prev_bad || vload(&sMisc[0]));
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (failed) break;
     if (tid == 0) {
       split_gemm(tmem, saddr(sA), C::A_PART, saddr(sBV), C::BV_PART, KV, NV, idv);
       tc_commit(mvol);
       pend_v = true;
+      par_v = (uint32_t)k & 1u;
     }
 
     // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
@@ -362,6 +402,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
       split_gemm(tmem + NV, saddr(sA), C::A_PART, saddr(sBL), C::BL_PART, KL, NL, idl);
       tc_commit(mlift);
       pend_l = true;
+      par_l = (uint32_t)k & 1u;
     }
 
     // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
@@ -417,29 +458,17 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
         }
       }
     }
-    fence_async_smem();  // the slot writes become visible to the bulk stores
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    failed = consumers_any<CW>(!ldone);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (failed) break;
-    if (tid == 0) {
-      const uint32_t nbd = tail0 * 4;
-      if (nbd) {
-        bulk_s2g(A.uhi_out + slot0, sHi, nbd);
-        bulk_s2g(A.ulo_out + slot0, sLo, nbd);
-        bulk_s2g(A.resu + slot0, sRe, nbd);
-      }
-      bulk_commit();
-      bulk_wait_read_all();  // the slot may be refilled once the stores have read it
-      mbar_arrive(&empty[s]);
-    }
+    fence_async_smem();  // the slot writes become visible to the producer's bulk stores
+    prev_bad = !ldone;
+    mbar_arrive(&done[s]);
   }
+  if (!failed) failed = consumers_any<CW>(prev_bad);
   if (failed && tid == 0) {
     atomicExch(A.status, kStatusTimeoutCode);
     *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
     // MMAs committed for tile k must complete before TMEM is freed (each wait is bounded)
-    if (pend_v) mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
-    if (pend_l) mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
+    if (pend_v) mbar_wait_bounded(mvol, par_v, kSpinLimit);
+    if (pend_l) mbar_wait_bounded(mlift, par_l, kSpinLimit);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   asm volatile("bar.sync 1, %0;" ::"n"(32 * CW) : "memory");
@@ -474,15 +503,24 @@ bool launch_tcm_n(const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *
 
 template <int N>
 void prepare_tcm_cw(int cw) {
-  if (cw == 16)
-    tcm_attr<N, 16>();
-  else
-    tcm_attr<N, 8>();
+  switch (cw) {
+    case 8: tcm_attr<N, 8>(); break;
+    case 12: tcm_attr<N, 12>(); break;
+    case 16: tcm_attr<N, 16>(); break;
+    case 20: tcm_attr<N, 20>(); break;
+    default: break;
+  }
 }
 
 template <int N>
 bool launch_tcm_cw(const MixedArgs &A, int cw, int num_sms, cudaStream_t st, LaunchInfo *info) {
-  return cw == 16 ? launch_tcm_n<N, 16>(A, num_sms, st, info) : launch_tcm_n<N, 8>(A, num_sms, st, info);
+  switch (cw) {
+    case 8: return launch_tcm_n<N, 8>(A, num_sms, st, info);
+    case 12: return launch_tcm_n<N, 12>(A, num_sms, st, info);
+    case 16: return launch_tcm_n<N, 16>(A, num_sms, st, info);
+    case 20: return launch_tcm_n<N, 20>(A, num_sms, st, info);
+    default: return false;
+  }
 }
 
 template <int N>
