@@ -41,7 +41,7 @@ bool tcm_supported(int N);
 int tcm_tile_elems();
 void tcm_pack_operands(int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
                        std::vector<uint16_t> &out);
-// consumer_warps 8, 12, 16 or 20 (2 to 5 threads per element)
+// consumer_warps 8 or 16 (2 or 4 threads per element)
 void prepare_rhs_tcm(int N, int consumer_warps);  // attributes, before any stream capture
 bool launch_rhs_tcm(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st, LaunchInfo *info);
 template <typename T>

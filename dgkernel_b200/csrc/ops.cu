@@ -456,8 +456,7 @@ struct MixedOp : Op {
       throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the tensor-core mixed stage is built for orders 1..4");
     if (mma) {
       warps = R.flag("warps", 16);
-      require(warps == 8 || warps == 12 || warps == 16 || warps == 20,
-              R.kname + ": warps must be 8, 12, 16 or 20 with mma=1");
+      require(warps == 8 || warps == 16, R.kname + ": warps must be 8 or 16 with mma=1");
     } else {
       warps = R.flag("warps", 11);
       require(warps == 4 || warps == 8 || warps == 11, R.kname + ": warps must be 4, 8 or 11");

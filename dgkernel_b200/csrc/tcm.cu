@@ -6,7 +6,8 @@
 // FP32.  The two products per element, D{r,s,t} dw and LIFT flux, run as GEMMs over tiles of 128 elements:
 //
 //   acc_V[e][3i+d] = sum_j dw[e][j] D_d[i][j]      M = 128 elements, N = rup16(3 Np), K = rup16(Np)
-//   acc_L[e][i]    = sum_m fl[e][m] LIFT[i][m]     M = 128 elements, N = rup16(Np),   K = rup16(4 Nfp)
+//   acc_L[e][i]    = sum_m fl[e][m] LIFT[i][m]     M = 128 elements, N = rup16(Np),   K = 4 rup8(Nfp)
+//                                                  (face-major K, each face's points padded to 8)
 //
 // with elements on the MMA's M dimension, so that TMEM lane e holds element e's outputs and the threads that
 // own element e read them back.  Every operand is split into three BF16 parts, x = x0 + x1 + x2 (x0 = bf16(x),
@@ -16,7 +17,7 @@
 //
 // CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry and connectivity into a
 // 2-slot ring with 1-D bulk copies; CW consumer warps hold CW / 4 threads per element (warps w, w + 4, ... share
-// the TMEM lane quarter w mod 4 and split the element's nodes and face points in 8-wide chunks).  Per tile: the
+// the TMEM lane quarter w mod 4 and split the element's nodes in 8-wide chunks and its faces).  Per tile: the
 // threads write the split dw into the A buffer (K-major canonical layout), one thread issues the volume MMAs,
 // the threads gather the neighbour traces and form the flux meanwhile, write it into the same A buffer once
 // the volume MMAs have completed, one thread issues the LIFT MMAs, and the threads read both accumulators from
@@ -45,7 +46,9 @@ template <int N>
 struct TmCfg {
   using O = Order<N>;
   static constexpr int NP = O::NP, NFP = O::NFP, NF = O::NF;
-  static constexpr int KV = rup16(NP), KL = rup16(NF), NV = rup16(3 * NP), NL = rup16(NP);
+  // LIFT's K runs face-major, each face padded to KF columns: column f KF + p holds face f's point p
+  static constexpr int KF = (NFP + 7) & ~7;
+  static constexpr int KV = rup16(NP), KL = rup16(4 * KF), NV = rup16(3 * NP), NL = rup16(NP);
   static constexpr int KA = KV > KL ? KV : KL;
   static constexpr uint32_t BV_PART = (uint32_t)NV * KV * 2, BL_PART = (uint32_t)NL * KL * 2;
   static constexpr uint32_t A_PART = (uint32_t)kTmTE * KA * 2;
@@ -58,15 +61,15 @@ struct TmCfg {
   static constexpr uint32_t OFF_SLOT = OFF_A + 3 * A_PART, OFF_BARY = OFF_SLOT + 2 * SLOT_B;
   static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;  // full[2], done[2], vol, lift
   static constexpr uint32_t OFF_MISC = OFF_BARS + 6 * 8;                  // abort flag, TMEM base
-  static constexpr uint32_t OFF_FMASK = OFF_MISC + 16;
-  static constexpr uint32_t OFF_FTAB = OFF_FMASK + ((NF + 15) & ~15);
+  static constexpr uint32_t OFF_FMASK = (OFF_MISC + 16 + 15) & ~15u;
+  static constexpr uint32_t OFF_FTAB = OFF_FMASK + ((NF + 15) & ~15);  // face-order rows of 16 bytes
   static constexpr uint32_t CONST_BYTES = 3 * BV_PART + 3 * BL_PART;  // the packed operand buffer
-  static_assert(3 * NP <= 256 && NP <= 128, "tile shapes");
+  static_assert(3 * NP <= 256 && NP <= 128 && NFP <= 16, "tile shapes");
 };
 
 template <int N>
 __host__ __device__ constexpr uint32_t tm_smem(int ncodes) {
-  return TmCfg<N>::OFF_FTAB + (((uint32_t)ncodes * TmCfg<N>::NFP + 15u) & ~15u);
+  return TmCfg<N>::OFF_FTAB + (uint32_t)ncodes * 16u;
 }
 
 // Round a pair to BF16 (one paired conversion): the packed bits, low half = x, and the residuals x - bf16(x).
@@ -141,11 +144,16 @@ __device__ __forceinline__ int vload(const int *p) { return *reinterpret_cast<co
 
 }  // namespace
 
-// CW = 8, 12, 16 or 20 consumer warps: CW / 4 threads per element.
-template <int N, int CW>
+// CW = 8 or 16 consumer warps: CW / 4 = 2 or 4 threads per element, each owning 4 / (CW / 4) faces.
+// CONS: conservative form (w = u^2/2).
+template <int N, int CW, bool CONS>
 __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const MixedArgs A) {
   using C = TmCfg<N>;
   constexpr int TPE = CW / 4;  // threads per element
+  constexpr int FPT = 4 / TPE; // faces per thread
+  constexpr int KF = C::KF;
+  static_assert(TPE == 2 || TPE == 4, "2 or 4 threads per element");
+  constexpr bool cons = CONS;
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, KV = C::KV, KL = C::KL, NV = C::NV, NL = C::NL;
   constexpr int TE = kTmTE;
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -167,7 +175,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   }
   for (int x = tid; x < NP * 3; x += blockDim.x) sBary[x] = A.bary[x];
   for (int x = tid; x < NF; x += blockDim.x) sFm[x] = (uint8_t)A.fmask[x];
-  for (int x = tid; x < A.ncodes * NFP; x += blockDim.x) sFt[x] = A.ftab[x];
+  for (int x = tid; x < A.ncodes * 16; x += blockDim.x) sFt[x] = (x & 15) < NFP ? A.ftab[(x >> 4) * NFP + (x & 15)] : 0;
   if (tid == 0) {
     for (int b = 0; b < 6; ++b) mbar_init(&full[b], (b == 2 || b == 3) ? 32 * CW : 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -264,7 +272,6 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const float a = A.a, dt = A.dt;
   const double b = A.b;
-  const int cons = A.conservative;
   const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
   const int ncodes = A.ncodes;
   const uint32_t idv = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
@@ -294,35 +301,37 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     const int ee = valid ? e : 0;
     const float *hi = sHi + ee * NP;
     const float *lo = sLo + ee * NP;
-    const float cr = sGeo[ee * kMixedGeoWords], cs = sGeo[ee * kMixedGeoWords + 1], ct = sGeo[ee * kMixedGeoWords + 2];
+    const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords);
+    const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords + 4);
+    const float cr = g0.x, cs = g0.y, ct = g0.z;
     const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
 
-    // ---- neighbour traces for this thread's face points, loaded first so that their latency overlaps dw ----
-    constexpr int NCL = (KL / 8 + TPE - 1) / TPE;  // flux chunks per thread
-    float fl[NCL][8];                               // uP, then the flux
+    // ---- neighbour traces of this thread's faces, loaded first so that their latency overlaps dw ----
+    float fl[FPT][KF];  // uP, then the flux; face h FPT + ff, point p
     {
       bool bad = false;
       const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
 #pragma unroll
-      for (int cc = 0; cc < NCL; ++cc) {
-        const int c = h + TPE * cc;
+      for (int ff = 0; ff < FPT; ++ff) {
+        const int f = h * FPT + ff;
+        const uint32_t nb = (uint32_t)sCon[ee * kMixedConnWords + f];
+        const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
+        const uint4 row = *reinterpret_cast<const uint4 *>(sFt + cd * 16);  // this face's point order
+        const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
+        const uint8_t *fm = sFm + f * NFP;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int m = 8 * c + q;
+        for (int p = 0; p < KF; ++p) {
           float v = 0.f;
-          if (got && c < KL / 8 && m < NF) {
-            const int f = m / NFP, p = m - f * NFP;
-            const uint32_t nb = (uint32_t)sCon[ee * kMixedConnWords + f];
-            const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
-            const uint32_t idx = nb + sFt[cd * NFP + p];
+          if (p < NFP && got) {
+            const uint32_t idx = nb + ((rw[p >> 2] >> (8 * (p & 3))) & 0xffu);
             const uint32_t loc = idx - (uint32_t)slot0;
             const bool ins = loc < (uint32_t)slotn;
             const bool okg = idx < n_u32;
             bad |= valid && !ins && !okg;
-            const float *src = ins ? sHi + loc : (okg ? A.uhi_in + idx : hi + sFm[m]);
+            const float *src = ins ? sHi + loc : (okg ? A.uhi_in + idx : hi + fm[p]);
             v = *src;
           }
-          fl[cc][q] = v;
+          fl[ff][p] = v;
         }
       }
       if (bad) atomicExch(A.status, kStatusBadGather);
@@ -367,18 +376,15 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
 
     // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
 #pragma unroll
-    for (int cc = 0; cc < NCL; ++cc) {
-      const int c = h + TPE * cc;
+    for (int ff = 0; ff < FPT; ++ff) {
+      const int f = h * FPT + ff;
+      const float g = f == 0 ? g0.w : f == 1 ? g1.x : f == 2 ? g1.y : g1.z, ga = fabsf(g);
+      const uint8_t *fm = sFm + f * NFP;
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int m = 8 * c + q;
-        if (c < KL / 8 && m < NF) {
-          const int f = m / NFP;
-          const float uM = hi[sFm[m]], uP = fl[cc][q];
-          const float g = sGeo[ee * kMixedGeoWords + 3 + f], ga = fabsf(g);
-          const float d = uM - uP;
-          fl[cc][q] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
-        }
+      for (int p = 0; p < NFP; ++p) {
+        const float uM = hi[fm[p]], uP = fl[ff][p];
+        const float d = uM - uP;
+        fl[ff][p] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
       }
     }
 
@@ -388,9 +394,15 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (vdone && valid) {
 #pragma unroll
-      for (int cc = 0; cc < NCL; ++cc) {
-        const int c = h + TPE * cc;
-        if (c < KL / 8) store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, fl[cc]);
+      for (int ff = 0; ff < FPT; ++ff) {
+        const int f = h * FPT + ff;
+#pragma unroll
+        for (int cq = 0; cq < KF / 8; ++cq) {
+          float v[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) v[q] = fl[ff][8 * cq + q];
+          store_split8(sA + (size_t)kmaj(e, f * KF + 8 * cq, TE) * 2, C::A_PART, v);
+        }
       }
     }
     fence_async_smem();
@@ -478,24 +490,25 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
 
 namespace {
 
-template <int N, int CW>
+template <int N, int CW, bool CONS>
 void tcm_attr() {
   static bool done[64] = {};
   int dev = 0;
   cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
   if (dev >= 0 && dev < 64 && done[dev]) return;
-  cuda_check(cudaFuncSetAttribute(rhs_stage_tcm_kernel<N, CW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024),
+  cuda_check(cudaFuncSetAttribute(rhs_stage_tcm_kernel<N, CW, CONS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  227 * 1024),
              "tcm kernel smem attribute");
   if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
-template <int N, int CW>
+template <int N, int CW, bool CONS>
 bool launch_tcm_n(const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info) {
   const uint32_t smem = tm_smem<N>(A.ncodes);
   if (smem > 227u * 1024u) return false;
-  tcm_attr<N, CW>();
+  tcm_attr<N, CW, CONS>();
   const int grid = std::max(1, std::min(num_sms, A.ntiles));
-  rhs_stage_tcm_kernel<N, CW><<<grid, 32 * (CW + 1), smem, st>>>(A);
+  rhs_stage_tcm_kernel<N, CW, CONS><<<grid, 32 * (CW + 1), smem, st>>>(A);
   cuda_check(cudaGetLastError(), "rhs_stage_tcm_kernel launch");
   if (info) *info = LaunchInfo{grid, 32 * (CW + 1), (int)smem, 1};
   return true;
@@ -503,24 +516,22 @@ bool launch_tcm_n(const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *
 
 template <int N>
 void prepare_tcm_cw(int cw) {
-  switch (cw) {
-    case 8: tcm_attr<N, 8>(); break;
-    case 12: tcm_attr<N, 12>(); break;
-    case 16: tcm_attr<N, 16>(); break;
-    case 20: tcm_attr<N, 20>(); break;
-    default: break;
+  if (cw == 8) {
+    tcm_attr<N, 8, false>();
+    tcm_attr<N, 8, true>();
+  } else if (cw == 16) {
+    tcm_attr<N, 16, false>();
+    tcm_attr<N, 16, true>();
   }
 }
 
 template <int N>
 bool launch_tcm_cw(const MixedArgs &A, int cw, int num_sms, cudaStream_t st, LaunchInfo *info) {
-  switch (cw) {
-    case 8: return launch_tcm_n<N, 8>(A, num_sms, st, info);
-    case 12: return launch_tcm_n<N, 12>(A, num_sms, st, info);
-    case 16: return launch_tcm_n<N, 16>(A, num_sms, st, info);
-    case 20: return launch_tcm_n<N, 20>(A, num_sms, st, info);
-    default: return false;
-  }
+  const bool cons = A.conservative != 0;
+  if (cw == 8) return cons ? launch_tcm_n<N, 8, true>(A, num_sms, st, info) : launch_tcm_n<N, 8, false>(A, num_sms, st, info);
+  if (cw == 16)
+    return cons ? launch_tcm_n<N, 16, true>(A, num_sms, st, info) : launch_tcm_n<N, 16, false>(A, num_sms, st, info);
+  return false;
 }
 
 template <int N>
@@ -541,8 +552,10 @@ void tcm_pack_n(const double *Dr, const double *Ds, const double *Dt, const doub
   for (int i = 0; i < NP; ++i)
     for (int d = 0; d < 3; ++d)
       for (int j = 0; j < NP; ++j) put(0, pv, NV, 3 * i + d, j, D[d][i * NP + j]);
+  constexpr int NFP = C::NFP, KF = C::KF;
   for (int i = 0; i < NP; ++i)
-    for (int m = 0; m < NF; ++m) put(3 * pv, pl, NL, i, m, LIFT[(size_t)i * NF + m]);
+    for (int f = 0; f < 4; ++f)
+      for (int q = 0; q < NFP; ++q) put(3 * pv, pl, NL, i, f * KF + q, LIFT[(size_t)i * NF + f * NFP + q]);
 }
 
 }  // namespace
