@@ -1,7 +1,7 @@
 // Mixed-precision stage with its element-local products on the tensor cores (tcgen05, sm_100a), orders 1..4.
 //
 // Same arithmetic contract as rhs_stage_mixed_kernel (mixed.cu): the state is a compensated FP32 pair
-// (u = hi + lo), the residual FP32, the update FP64; the derivative operand is w minus its linear vertex
+// (u = hi + lo), the residual FP32; the derivative operand is w minus its linear vertex
 // interpolant (w = u or u^2/2), whose exact derivative is added back; the Lax-Friedrichs flux is formed in
 // FP32.  The two products per element, D{r,s,t} dw and LIFT flux, run as GEMMs over tiles of 128 elements:
 //
@@ -21,7 +21,7 @@
 // threads write the split dw into the A buffer (K-major canonical layout), one thread issues the volume MMAs,
 // the threads gather the neighbour traces and form the flux meanwhile, write it into the same A buffer once
 // the volume MMAs have completed, one thread issues the LIFT MMAs, and the threads read both accumulators from
-// TMEM and finish the stage in FP64 into the slot, which the producer writes back with bulk stores before it
+// TMEM and finish the stage (the compensated update in error-free FP32 arithmetic) into the slot, which the producer writes back with bulk stores before it
 // refills it.  Constant operands (D and LIFT, split) stay in shared memory for the whole launch.  Every wait is bounded; a failed wait sets the status
 // word and the CTA leaves after draining its copies and MMAs; TMEM is always freed.
 #include <cuda_bf16.h>
@@ -123,6 +123,20 @@ __device__ __forceinline__ void tmem_ld24(uint32_t t0, float (&v)[24]) {
       : "memory");
 #pragma unroll
   for (int j = 0; j < 24; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// (hn, ln) = (hi + lo) + b rn in error-free FP32 arithmetic, with b = bh + bl: the product by FMA residuals,
+// the sums by Knuth's two-sum; about 47 significant bits, like an FP64 update rounded back to the pair.
+__device__ __forceinline__ void stage_update(float hi, float lo, float rn, float bh, float bl, float &hn, float &ln) {
+  const float p = bh * rn;
+  const float ep = fmaf(bl, rn, fmaf(bh, rn, -p));  // b rn = p + ep
+  const float s = hi + p;
+  const float bb = s - hi;
+  const float es = (hi - (s - bb)) + (p - bb);      // hi + p = s + es exactly
+  const float t = lo + (ep + es);
+  hn = s + t;
+  const float bt = hn - s;
+  ln = (s - (hn - bt)) + (t - bt);  // s + t = hn + ln exactly
 }
 
 // One GEMM of the split products: 6 MMAs per 16-wide K step into the accumulator at `acc`.
@@ -271,7 +285,8 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   const int e = (warp & 3) * 32 + lane, h = TPE - 1 - (warp >> 2);
   const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const float a = A.a, dt = A.dt;
-  const double b = A.b;
+  // b as an unevaluated pair of floats (b = bh + bl to about 2^-48) for the FP32 compensated update
+  const float bh = __double2float_rn(A.b), bl = __double2float_rn(A.b - (double)bh);
   const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
   const int ncodes = A.ncodes;
   const uint32_t idv = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
@@ -436,7 +451,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
       }
     }
 
-    // ---- LIFT accumulator, the stage update in FP64, the slot written back ----
+    // ---- LIFT accumulator and the compensated stage update into the slot ----
     const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
     if (ldone) pend_l = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -454,9 +469,8 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
             if (i < NP && valid) {
               const int o = e * NP + i;
               const float rn = fmaf(dt, lf[q], t0[cc][q]);
-              const double un = ((double)hi[i] + (double)lo[i]) + b * (double)rn;
-              const float hn = __double2float_rn(un);
-              const float ln = __double2float_rn(un - (double)hn);
+              float hn, ln;
+              stage_update(hi[i], lo[i], rn, bh, bl, hn, ln);
               sHi[o] = hn;
               sLo[o] = ln;
               sRe[o] = rn;
