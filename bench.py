@@ -209,16 +209,29 @@ def run_ensemble(args, world, rank, local):
     g = E.capture_steps(2)
     reps = max(1, args.steps // 10)
     E.run_graph(g, 1)
+    # The instances are inviscid and unlimited: past t ~ 0.17 (about 200 stages) the finest ones form shocks and
+    # leave the stable range.  The timed stages therefore run in blocks of at most 100 (10 graph replays), each
+    # from the same smooth state restored on the device outside the timed region (stage work does not depend on
+    # the values).
+    E.runner.ExecuteKernel("joinState")  # the FP64 array u keeps the smooth start (the stages touch only hi, lo)
     barrier(world)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    elapsed, ok = 0.0, True
     with ClockSampler(local) as clk:
-        e0.record(stream)
-        E.run_graph(g, reps)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1) / (10 * reps), world)
-    ok = bool(np.isfinite(E.get("u")).all())
+        left = reps
+        while left > 0:
+            nrep = min(10, left)
+            E.runner.ExecuteKernel("splitState")
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            E.run_graph(g, nrep)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            elapsed += e0.elapsed_time(e1)
+            left -= nrep
+        ok = bool(np.isfinite(E.get("u")).all())
+    ms = max_over_ranks(elapsed / (10 * reps), world)
     if rank == 0:
         out = {"metric": "DOF-stage-updates/s, batching form (256 order-3 instances)", "value": world * E.dofs / (ms * 1e-3),
                "unit": UNIT, "n_gpus": world, "steps": 10 * reps, "warmup": 10, "ms_per_step": ms,
@@ -228,6 +241,8 @@ def run_ensemble(args, world, rank, local):
                                       f"n_i ~ U{{6..24}} (K = {E.K}), one partition per instance, seeded "
                                       f"random-mode u0 per instance; one step = one LSERK4 stage of all instances",
                           "launch": "one persistent mixed-stage launch per stage, 10-stage CUDA graph replayed",
+                          "timed_blocks": "blocks of <= 100 stages, each from the same smooth state (restored "
+                                          "untimed): the inviscid instances form shocks after ~200 stages",
                           "tuned_shape": best, "setup_s": setup_s, "finite": ok},
                "clocks": clk.summary(), "gpu_launches": 10 * reps}
         print(json.dumps(out), flush=True)

@@ -9,8 +9,10 @@ Timing runs stage 0 of the LSERK4 scheme with dt = 0 from a step boundary: the r
 state is rewritten unchanged, so tuning leaves the solution where it was (the next real stage 0 ignores the
 residual).  Every candidate computes the same arithmetic per element, so the choice changes speed only.
 
-Candidates of the mixed stage: consumer warps per CTA (4, 8, 11) and ring slots (as many as shared memory
-holds, or 6).  The plain stages have one launch shape per order and are not tuned.
+Candidates of the mixed stage: its FP32-FMA form with 4, 8 or 11 consumer warps per CTA and a ring of as many
+slots as shared memory holds, or 6; and, at orders 1..4, its tensor-core form with 2 or 4 threads per element
+(8 or 16 consumer warps).  The two forms round differently (both within the mixed stage's error bound); launch
+shapes of one form give the same bits.  The plain stages have one launch shape per order and are not tuned.
 """
 from __future__ import annotations
 
@@ -21,7 +23,13 @@ from typing import Callable, Dict, List, Optional
 
 from .burgers import RK4B
 
-MIXED_CANDIDATES: List[Dict] = [{"warps": w, "ring": r} for w in (11, 8, 4) for r in (None, 6)]
+MIXED_CANDIDATES: List[Dict] = [{"warps": w, "ring": r, "mma": False} for w in (11, 8, 4) for r in (None, 6)]
+TCM_CANDIDATES: List[Dict] = [{"warps": w, "ring": None, "mma": True} for w in (16, 8)]
+
+
+def candidates_for(problem) -> List[Dict]:
+    """The launch shapes the tuner tries for this problem's stage operator."""
+    return MIXED_CANDIDATES + (TCM_CANDIDATES if problem.N <= 4 else [])
 
 
 def default_cache_path() -> str:
@@ -109,7 +117,7 @@ def autotune(problem, cache_path: Optional[str] = None, stages: int = 8, candida
         r.Sync()
         return (time.perf_counter() - t0) * 1e3 / stages
 
-    best, times = search(candidates or MIXED_CANDIDATES, measure)
+    best, times = search(candidates or candidates_for(problem), measure)
     problem.build_stage(**best)
     r.Sync()
     cache[key] = {"best": best, "ms_per_stage": times, "when": time.strftime("%Y-%m-%d %H:%M:%S")}

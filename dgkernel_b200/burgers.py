@@ -218,9 +218,12 @@ class _TetBurgers:
             args.append(f"ring={ring}")
         return "rhsStageMixed(" + ",".join(args) + ")"
 
-    def build_stage(self, warps=None, ring=None):
-        """(Re)build the stage operator, optionally with a given launch shape."""
-        self.shape = {"warps": warps, "ring": ring}
+    def build_stage(self, warps=None, ring=None, mma=None):
+        """(Re)build the stage operator, optionally with a given launch shape (and, for the mixed stage, the
+        product path: mma=True puts the element-local products on the tensor cores)."""
+        if mma is not None:
+            self.mma = bool(mma)
+        self.shape = {"warps": warps, "ring": ring, "mma": bool(getattr(self, "mma", None))}
         self.runner.BuildKernel(self.op_id(warps, ring), "rhsStage")
 
     def set_sensor(self, sensor: str, params=None):

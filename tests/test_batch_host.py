@@ -53,3 +53,14 @@ def test_autotune_search_and_cache(tmp_path):
     assert T.load_cache(path) == {}
     os.environ.pop("DGK_TUNE_CACHE", None)
     assert T.default_cache_path().endswith(os.path.join("dgkernel_b200", "tune.json"))
+
+
+def test_autotune_candidates_by_order():
+    """Orders 1..4 also try the tensor-core form of the mixed stage; order 5 has only the FP32-FMA form."""
+    class P:
+        def __init__(self, N):
+            self.N = N
+    c4, c5 = T.candidates_for(P(4)), T.candidates_for(P(5))
+    assert any(c["mma"] for c in c4) and not any(c["mma"] for c in c5)
+    assert all(c["warps"] in (8, 16) for c in c4 if c["mma"])
+    assert c5 == T.MIXED_CANDIDATES

@@ -61,8 +61,9 @@ def test_autotune_keeps_state_and_results(tmp_path):
     B = BurgersEnsemble(3, SIZES)
     before = B.get("u")
     best = T.autotune(B, cache_path=str(tmp_path / "tune.json"), stages=2)
-    assert best in T.MIXED_CANDIDATES
+    assert best in T.candidates_for(B)
     assert np.array_equal(B.get("u"), before)  # tuning stages run with dt = 0
+    A.build_stage(**best)  # the same form and launch shape: the same bits
     A.run_stages(10)
     B.run_stages(10)
     assert np.array_equal(A.get("u"), B.get("u"))
