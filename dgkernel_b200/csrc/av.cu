@@ -98,6 +98,7 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_prep_kernel(const AvArgs
     if (act) {
       const double *ue = su + e * NP;
       double uh = 0.0, ur = 0.0, us = 0.0, ut = 0.0;
+#pragma unroll 5
       for (int j = 0; j < NP; ++j) {
         const double v = ue[j];
         uh = fma(sVi[i * NP + j], v, uh);
@@ -109,6 +110,7 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_prep_kernel(const AvArgs
       for (int d = 0; d < 3; ++d) {
         double q = A.geo[d][nb + i] * ur + A.geo[3 + d][nb + i] * us + A.geo[6 + d][nb + i] * ut;
         const double *fl = sfl + (d * TE + e) * NF;
+#pragma unroll 6
         for (int m = 0; m < NF; ++m) q = fma(sL[i * NF + m], fl[m], q);
         A.q[d][nb + i] = q;
       }
@@ -117,6 +119,7 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_prep_kernel(const AvArgs
     // sensor: energy ratio, features, PP activation
     if (act && i == 0) {
       double tot = 0.0, hi = 0.0;
+#pragma unroll 5
       for (int j = 0; j < NP; ++j) {
         const double v = suh[e * NP + j];
         tot += v * v;
@@ -236,6 +239,7 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_rhs_kernel(const AvArgs 
     if (act) {
       const double *ue = su + e * NP;
       double ur = 0.0, us = 0.0, ut = 0.0;
+#pragma unroll 5
       for (int j = 0; j < NP; ++j) {
         ur = fma(sDr[i * NP + j], ue[j], ur);
         us = fma(sDs[i * NP + j], ue[j], us);
@@ -251,7 +255,8 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_rhs_kernel(const AvArgs 
         for (int d = 0; d < 3; ++d) {
           const double *qd = sq + (d * TE + e) * NP;
           double qr = 0.0, qs = 0.0, qt = 0.0;
-          for (int j = 0; j < NP; ++j) {
+    #pragma unroll 5
+      for (int j = 0; j < NP; ++j) {
             qr = fma(sDr[i * NP + j], qd[j], qr);
             qs = fma(sDs[i * NP + j], qd[j], qs);
             qt = fma(sDt[i * NP + j], qd[j], qt);
@@ -262,6 +267,7 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_rhs_kernel(const AvArgs 
       }
       const double *fl = sfl + e * NF;
       double lift = 0.0;
+#pragma unroll 6
       for (int m = 0; m < NF; ++m) lift = fma(sL[i * NF + m], fl[m], lift);
       rhs += lift;
       const double r = a * A.resu[nb + i] + dt * rhs;
