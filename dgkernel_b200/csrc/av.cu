@@ -136,6 +136,8 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_prep_kernel(const AvArgs
     if (act) {
       const double f = suh[e * NP + i] * sfmax[e];
       suh[e * NP + i] = f;
+      // FP32 copy for the network, in the flux buffer (dead once q is written)
+      reinterpret_cast<float *>(sfl)[e * NP + i] = (float)f;
       if (A.feat_out) A.feat_out[tl.feat_base + (int64_t)e * NP + i] = (float)f;
     }
     __syncthreads();
@@ -145,16 +147,27 @@ __global__ void __launch_bounds__(AvCfg<N>::THREADS) av_prep_kernel(const AvArgs
                    *b3 = w3 + kHid;
       if (act)
         for (int o = i; o < kHid; o += NP) {
-          float s = __half2float(b1[o]);
-          for (int j = 0; j < NP; ++j) s = fmaf(__half2float(W1[o * NP + j]), (float)suh[e * NP + j], s);
-          sh1[e * kHid + o] = tanhf(s);
+          // FP16 weights, FP32 sums in two chains over the FP32 features
+          const float *x = reinterpret_cast<const float *>(sfl) + e * NP;
+          float s0 = __half2float(b1[o]), s1 = 0.f;
+#pragma unroll
+          for (int j = 0; j + 1 < NP; j += 2) {
+            s0 = fmaf(__half2float(W1[o * NP + j]), x[j], s0);
+            s1 = fmaf(__half2float(W1[o * NP + j + 1]), x[j + 1], s1);
+          }
+          if (NP & 1) s0 = fmaf(__half2float(W1[o * NP + NP - 1]), x[NP - 1], s0);
+          sh1[e * kHid + o] = tanhf(s0 + s1);
         }
       __syncthreads();
       if (act)
         for (int o = i; o < kHid; o += NP) {
-          float s = __half2float(b2[o]);
-          for (int j = 0; j < kHid; ++j) s = fmaf(__half2float(W2[o * kHid + j]), sh1[e * kHid + j], s);
-          sh2[e * kHid + o] = tanhf(s);
+          float s0 = __half2float(b2[o]), s1 = 0.f;
+#pragma unroll
+          for (int j = 0; j < kHid; j += 2) {
+            s0 = fmaf(__half2float(W2[o * kHid + j]), sh1[e * kHid + j], s0);
+            s1 = fmaf(__half2float(W2[o * kHid + j + 1]), sh1[e * kHid + j + 1], s1);
+          }
+          sh2[e * kHid + o] = tanhf(s0 + s1);
         }
       __syncthreads();
       if (act && i == 0) {
