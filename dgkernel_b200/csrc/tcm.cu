@@ -279,9 +279,9 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     return;
   }
 
-  // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h of its nodes and face
-  // points (8-wide chunks h, h + TPE, ...), h = TPE - 1 - w / 4 so that the warps of thread 0 (which issues the
-  // MMAs) take the shares with fewer chunks
+  // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h of its nodes (8-wide
+  // chunks h, h + TPE, ...) and faces (h FPT .. h FPT + FPT - 1), h = TPE - 1 - w / 4 so that the warps of
+  // thread 0 (which issues the MMAs) take the node shares with fewer chunks
   const int e = (warp & 3) * 32 + lane, h = TPE - 1 - (warp >> 2);
   const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   const float a = A.a, dt = A.dt;
