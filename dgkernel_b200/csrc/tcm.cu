@@ -16,14 +16,16 @@
 // rounding (the dropped terms are below 2^-24 of the product).
 //
 // CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry and connectivity into a
-// 2-slot ring with 1-D bulk copies; CW consumer warps hold CW / 4 threads per element (warps w, w + 4, ... share
-// the TMEM lane quarter w mod 4 and split the element's nodes in 8-wide chunks and its faces).  Per tile: the
-// threads write the split dw into the A buffer (K-major canonical layout), one thread issues the volume MMAs,
-// the threads gather the neighbour traces and form the flux meanwhile, write it into the same A buffer once
-// the volume MMAs have completed, one thread issues the LIFT MMAs, and the threads read both accumulators from
-// TMEM and finish the stage (the compensated update in error-free FP32 arithmetic) into the slot, which the producer writes back with bulk stores before it
-// refills it.  Constant operands (D and LIFT, split) stay in shared memory for the whole launch.  Every wait is bounded; a failed wait sets the status
-// word and the CTA leaves after draining its copies and MMAs; TMEM is always freed.
+// 2-slot ring with 1-D bulk copies and writes finished slots back with bulk stores; one MMA warp issues the
+// GEMMs; CW consumer warps hold CW / 4 threads per element (warps w, w + 4, ... share the TMEM lane quarter
+// w mod 4 and split the element's nodes in 8-wide chunks and its faces).  Per tile: the consumer threads write
+// the split dw into the A buffer (K-major canonical layout) and arrive on an mbarrier, on which the MMA warp
+// issues the volume MMAs; they form the flux meanwhile, write it into the same A buffer once the volume MMAs
+// have completed and arrive again for the LIFT MMAs; then they read both accumulators from TMEM and finish the
+// stage (the compensated update in error-free FP32 arithmetic) into the slot.  No barrier among the consumers
+// within a tile.  Constant operands (D and LIFT, split) stay in shared memory for the whole launch.  Every wait
+// is bounded; a failed wait sets the status word and the CTA leaves after draining its copies and MMAs; TMEM is
+// always freed.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -59,8 +61,9 @@ struct TmCfg {
   // shared-memory layout (bytes)
   static constexpr uint32_t OFF_BV = 0, OFF_BL = OFF_BV + 3 * BV_PART, OFF_A = OFF_BL + 3 * BL_PART;
   static constexpr uint32_t OFF_SLOT = OFF_A + 3 * A_PART, OFF_BARY = OFF_SLOT + 2 * SLOT_B;
-  static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;  // full[2], done[2], vol, lift
-  static constexpr uint32_t OFF_MISC = OFF_BARS + 6 * 8;                  // abort flag, TMEM base
+  // full[2], done[2], mvol, mlift, avol, alift
+  static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;
+  static constexpr uint32_t OFF_MISC = OFF_BARS + 8 * 8;  // abort flag, TMEM base
   static constexpr uint32_t OFF_FMASK = (OFF_MISC + 16 + 15) & ~15u;
   static constexpr uint32_t OFF_FTAB = OFF_FMASK + ((NF + 15) & ~15);  // face-order rows of 16 bytes
   static constexpr uint32_t CONST_BYTES = 3 * BV_PART + 3 * BL_PART;  // the packed operand buffer
@@ -94,18 +97,6 @@ __device__ __forceinline__ void store_split8(unsigned char *dst, uint32_t part_b
   *reinterpret_cast<uint4 *>(dst) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
   *reinterpret_cast<uint4 *>(dst + part_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
   *reinterpret_cast<uint4 *>(dst + 2 * part_bytes) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
-}
-
-// bar.red.or over the CW consumer warps (named barrier 1): every consumer thread gets the same answer.
-template <int CW>
-__device__ __forceinline__ bool consumers_any(bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.or.pred q, 1, %2, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
-      : "=r"(r)
-      : "r"((uint32_t)v), "n"(32 * CW)
-      : "memory");
-  return r != 0;
 }
 
 // 24 consecutive TMEM columns (three 8-column loads) of this warp's lanes under one wait.
@@ -161,7 +152,7 @@ __device__ __forceinline__ int vload(const int *p) { return *reinterpret_cast<co
 // CW = 8 or 16 consumer warps: CW / 4 = 2 or 4 threads per element, each owning 4 / (CW / 4) faces.
 // CONS: conservative form (w = u^2/2).
 template <int N, int CW, bool CONS>
-__global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const MixedArgs A) {
+__global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const MixedArgs A) {
   using C = TmCfg<N>;
   constexpr int TPE = CW / 4;  // threads per element
   constexpr int FPT = 4 / TPE; // faces per thread
@@ -174,8 +165,10 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   unsigned char *sBV = sm + C::OFF_BV, *sBL = sm + C::OFF_BL, *sA = sm + C::OFF_A;
   unsigned char *ring = sm + C::OFF_SLOT;
   double *sBary = reinterpret_cast<double *>(sm + C::OFF_BARY);
+  // full: slot filled (producer's copies); done: slot finished (every consumer thread); mvol / mlift: MMA group
+  // complete (tcgen05.commit); avol / alift: operand written into the A buffer (every consumer thread)
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *done = full + 2, *mvol = full + 4,
-           *mlift = full + 5;
+           *mlift = full + 5, *avol = full + 6, *alift = full + 7;
   int *sMisc = reinterpret_cast<int *>(sm + C::OFF_MISC);  // [0] abort flag, [1] TMEM base
   uint8_t *sFm = sm + C::OFF_FMASK, *sFt = sm + C::OFF_FTAB;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -191,7 +184,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   for (int x = tid; x < NF; x += blockDim.x) sFm[x] = (uint8_t)A.fmask[x];
   for (int x = tid; x < A.ncodes * 16; x += blockDim.x) sFt[x] = (x & 15) < NFP ? A.ftab[(x >> 4) * NFP + (x & 15)] : 0;
   if (tid == 0) {
-    for (int b = 0; b < 6; ++b) mbar_init(&full[b], (b == 2 || b == 3) ? 32 * CW : 1);
+    for (int b = 0; b < 8; ++b) mbar_init(&full[b], (b == 2 || b == 3 || b >= 6) ? 32 * CW : 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     sMisc[0] = 0;
   }
@@ -206,7 +199,7 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = (uint32_t)sMisc[1];
 
-  if (warp == CW) {
+  if (warp == CW + 1) {
     // producer, lane 0: streams this CTA's tiles through the 2-slot ring and writes each finished slot back.
     // Slot s holds tile k, then k + 2: once every consumer thread has arrived on done[s] for tile k, the slot's
     // hi, lo and resu go out with bulk stores (the ragged tail past the last full 16 bytes was written by the
@@ -279,6 +272,50 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     return;
   }
 
+  const uint32_t idv = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
+  const uint32_t idl = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NL >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
+  bool failed = false;
+  if (warp == CW) {
+    // MMA warp: once every consumer thread has written tile k's dw (avol), lane 0 issues the volume GEMM and
+    // commits it to mvol; once they have written the flux (alift), the LIFT GEMM to mlift.
+    int k = 0, kv = -1, kl = -1;  // last tiles whose volume / LIFT groups were committed
+    for (;; ++k) {
+      const int t = blockIdx.x + k * G;
+      if (t >= A.ntiles) break;
+      if (!mbar_wait_bounded(avol, (uint32_t)k & 1u, kSpinLimit) || vload(&sMisc[0])) {
+        failed = true;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (lane == 0) {
+        split_gemm(tmem, saddr(sA), C::A_PART, saddr(sBV), C::BV_PART, KV, NV, idv);
+        tc_commit(mvol);
+      }
+      kv = k;
+      __syncwarp();
+      if (!mbar_wait_bounded(alift, (uint32_t)k & 1u, kSpinLimit) || vload(&sMisc[0])) {
+        failed = true;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (lane == 0) {
+        split_gemm(tmem + NV, saddr(sA), C::A_PART, saddr(sBL), C::BL_PART, KL, NL, idl);
+        tc_commit(mlift);
+      }
+      kl = k;
+      __syncwarp();
+    }
+    if (failed) {
+      if (lane == 0) {
+        atomicExch(A.status, kStatusTimeoutCode);
+        *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
+      }
+      // committed groups must complete before TMEM is freed (each wait is bounded)
+      if (kv >= 0) mbar_wait_bounded(mvol, (uint32_t)kv & 1u, kSpinLimit);
+      if (kl >= 0) mbar_wait_bounded(mlift, (uint32_t)kl & 1u, kSpinLimit);
+    }
+  } else {
+
   // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h of its nodes (8-wide
   // chunks h, h + TPE, ...) and faces (h FPT .. h FPT + FPT - 1), h = TPE - 1 - w / 4 so that the warps of
   // thread 0 (which issues the MMAs) take the node shares with fewer chunks
@@ -289,13 +326,8 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
   const float bh = __double2float_rn(A.b), bl = __double2float_rn(A.b - (double)bh);
   const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
   const int ncodes = A.ncodes;
-  const uint32_t idv = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NV >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
-  const uint32_t idl = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NL >> 3) << 17) | ((uint32_t)(TE >> 4) << 24);
   // gathered indices fit 32 bits (the compact connectivity stores int32 bases)
   const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
-  bool failed = false, prev_bad = false;  // prev_bad: the previous tile's LIFT wait failed
-  bool pend_v = false, pend_l = false;  // (thread 0) MMA groups committed and not yet seen complete
-  uint32_t par_v = 0, par_l = 0;         // their mbarrier phases
   MTile tl_next{};
   if ((int)blockIdx.x < A.ntiles) tl_next = A.tiles[blockIdx.x];
   int k = 0;
@@ -377,16 +409,12 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
         store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, v);
       }
     }
-    fence_async_smem();
+    fence_async_smem();  // the A buffer is read by the tensor cores (async proxy)
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    failed = consumers_any<CW>(!got || prev_bad || vload(&sMisc[0]));
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (failed) break;
-    if (tid == 0) {
-      split_gemm(tmem, saddr(sA), C::A_PART, saddr(sBV), C::BV_PART, KV, NV, idv);
-      tc_commit(mvol);
-      pend_v = true;
-      par_v = (uint32_t)k & 1u;
+    mbar_arrive(avol);
+    if (!got || vload(&sMisc[0])) {
+      failed = true;
+      break;
     }
 
     // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
@@ -405,7 +433,6 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
 
     // the volume MMAs have read the A buffer (and written acc_V) once mvol completes
     const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
-    if (vdone) pend_v = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (vdone && valid) {
 #pragma unroll
@@ -422,14 +449,10 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
     }
     fence_async_smem();
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    failed = consumers_any<CW>(!vdone);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (failed) break;
-    if (tid == 0) {
-      split_gemm(tmem + NV, saddr(sA), C::A_PART, saddr(sBL), C::BL_PART, KL, NL, idl);
-      tc_commit(mlift);
-      pend_l = true;
-      par_l = (uint32_t)k & 1u;
+    mbar_arrive(alift);
+    if (!vdone) {
+      failed = true;
+      break;
     }
 
     // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
@@ -453,7 +476,6 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
 
     // ---- LIFT accumulator and the compensated stage update into the slot ----
     const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
-    if (ldone) pend_l = false;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
     if (ldone) {
@@ -484,20 +506,21 @@ __global__ void __launch_bounds__(32 * (CW + 1), 1) rhs_stage_tcm_kernel(const M
         }
       }
     }
+    if (!ldone) {
+      failed = true;
+      break;
+    }
     fence_async_smem();  // the slot writes become visible to the producer's bulk stores
-    prev_bad = !ldone;
     mbar_arrive(&done[s]);
   }
-  if (!failed) failed = consumers_any<CW>(prev_bad);
-  if (failed && tid == 0) {
+  if (failed && lane == 0) {
     atomicExch(A.status, kStatusTimeoutCode);
     *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
-    // MMAs committed for tile k must complete before TMEM is freed (each wait is bounded)
-    if (pend_v) mbar_wait_bounded(mvol, par_v, kSpinLimit);
-    if (pend_l) mbar_wait_bounded(mlift, par_l, kSpinLimit);
   }
+  }  // consumers
+  // consumers and the MMA warp: TMEM is freed once every load from it and every MMA into it is done
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-  asm volatile("bar.sync 1, %0;" ::"n"(32 * CW) : "memory");
+  asm volatile("bar.sync 1, %0;" ::"n"(32 * (CW + 1)) : "memory");
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmCols));
 }
@@ -522,9 +545,9 @@ bool launch_tcm_n(const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *
   if (smem > 227u * 1024u) return false;
   tcm_attr<N, CW, CONS>();
   const int grid = std::max(1, std::min(num_sms, A.ntiles));
-  rhs_stage_tcm_kernel<N, CW, CONS><<<grid, 32 * (CW + 1), smem, st>>>(A);
+  rhs_stage_tcm_kernel<N, CW, CONS><<<grid, 32 * (CW + 2), smem, st>>>(A);
   cuda_check(cudaGetLastError(), "rhs_stage_tcm_kernel launch");
-  if (info) *info = LaunchInfo{grid, 32 * (CW + 1), (int)smem, 1};
+  if (info) *info = LaunchInfo{grid, 32 * (CW + 2), (int)smem, 1};
   return true;
 }
 
