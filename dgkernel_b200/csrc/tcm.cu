@@ -315,208 +315,206 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       if (kl >= 0) mbar_wait_bounded(mlift, (uint32_t)kl & 1u, kSpinLimit);
     }
   } else {
+    // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h = TPE - 1 - w / 4 of
+    // its nodes (8-wide chunks h, h + TPE, ...) and faces (h FPT .. h FPT + FPT - 1)
+    const int e = (warp & 3) * 32 + lane, h = TPE - 1 - (warp >> 2);
+    const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const float a = A.a, dt = A.dt;
+    // b as an unevaluated pair of floats (b = bh + bl to about 2^-48) for the FP32 compensated update
+    const float bh = __double2float_rn(A.b), bl = __double2float_rn(A.b - (double)bh);
+    const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
+    const int ncodes = A.ncodes;
+    // gathered indices fit 32 bits (the compact connectivity stores int32 bases)
+    const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
+    MTile tl_next{};
+    if ((int)blockIdx.x < A.ntiles) tl_next = A.tiles[blockIdx.x];
+    int k = 0;
+    for (;; ++k) {
+      const int t = blockIdx.x + k * G;
+      if (t >= A.ntiles) break;
+      const int s = k & 1;
+      const MTile tl = tl_next;
+      if (t + G < A.ntiles) tl_next = A.tiles[t + G];  // the next descriptor's load overlaps this tile
+      const int ne = tl.nelem;
+      const bool valid = e < ne;
+      const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
+      float *sHi = reinterpret_cast<float *>(ring + (size_t)s * C::SLOT_B);
+      float *sLo = sHi + TE * NP;
+      float *sRe = sLo + TE * NP;
+      const float *sGeo = sRe + TE * NP;
+      const int *sCon = reinterpret_cast<const int *>(sGeo + TE * kMixedGeoWords);
+      const int ee = valid ? e : 0;
+      const float *hi = sHi + ee * NP;
+      const float *lo = sLo + ee * NP;
+      const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords);
+      const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords + 4);
+      const float cr = g0.x, cs = g0.y, ct = g0.z;
+      const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
 
-  // consumers: thread (warp w, lane l) owns element e = 32 (w mod 4) + l and the share h of its nodes (8-wide
-  // chunks h, h + TPE, ...) and faces (h FPT .. h FPT + FPT - 1), h = TPE - 1 - w / 4 so that the warps of
-  // thread 0 (which issues the MMAs) take the node shares with fewer chunks
-  const int e = (warp & 3) * 32 + lane, h = TPE - 1 - (warp >> 2);
-  const uint32_t lane_tmem = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  const float a = A.a, dt = A.dt;
-  // b as an unevaluated pair of floats (b = bh + bl to about 2^-48) for the FP32 compensated update
-  const float bh = __double2float_rn(A.b), bl = __double2float_rn(A.b - (double)bh);
-  const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
-  const int ncodes = A.ncodes;
-  // gathered indices fit 32 bits (the compact connectivity stores int32 bases)
-  const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
-  MTile tl_next{};
-  if ((int)blockIdx.x < A.ntiles) tl_next = A.tiles[blockIdx.x];
-  int k = 0;
-  for (;; ++k) {
-    const int t = blockIdx.x + k * G;
-    if (t >= A.ntiles) break;
-    const int s = k & 1;
-    const MTile tl = tl_next;
-    if (t + G < A.ntiles) tl_next = A.tiles[t + G];  // the next descriptor's load overlaps this tile
-    const int ne = tl.nelem;
-    const bool valid = e < ne;
-    const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
-    float *sHi = reinterpret_cast<float *>(ring + (size_t)s * C::SLOT_B);
-    float *sLo = sHi + TE * NP;
-    float *sRe = sLo + TE * NP;
-    const float *sGeo = sRe + TE * NP;
-    const int *sCon = reinterpret_cast<const int *>(sGeo + TE * kMixedGeoWords);
-    const int ee = valid ? e : 0;
-    const float *hi = sHi + ee * NP;
-    const float *lo = sLo + ee * NP;
-    const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords);
-    const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords + 4);
-    const float cr = g0.x, cs = g0.y, ct = g0.z;
-    const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
-
-    // ---- neighbour traces of this thread's faces, loaded first so that their latency overlaps dw ----
-    float fl[FPT][KF];  // uP, then the flux; face h FPT + ff, point p
-    {
-      bool bad = false;
-      const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
+      // ---- neighbour traces of this thread's faces, loaded first so that their latency overlaps dw ----
+      float fl[FPT][KF];  // uP, then the flux; face h FPT + ff, point p
+      {
+        bool bad = false;
+        const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
 #pragma unroll
-      for (int ff = 0; ff < FPT; ++ff) {
-        const int f = h * FPT + ff;
-        const uint32_t nb = (uint32_t)sCon[ee * kMixedConnWords + f];
-        const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
-        const uint4 row = *reinterpret_cast<const uint4 *>(sFt + cd * 16);  // this face's point order
-        const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
-        const uint8_t *fm = sFm + f * NFP;
+        for (int ff = 0; ff < FPT; ++ff) {
+          const int f = h * FPT + ff;
+          const uint32_t nb = (uint32_t)sCon[ee * kMixedConnWords + f];
+          const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
+          const uint4 row = *reinterpret_cast<const uint4 *>(sFt + cd * 16);  // this face's point order
+          const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
+          const uint8_t *fm = sFm + f * NFP;
 #pragma unroll
-        for (int p = 0; p < KF; ++p) {
-          float v = 0.f;
-          if (p < NFP && got) {
-            const uint32_t idx = nb + ((rw[p >> 2] >> (8 * (p & 3))) & 0xffu);
-            const uint32_t loc = idx - (uint32_t)slot0;
-            const bool ins = loc < (uint32_t)slotn;
-            const bool okg = idx < n_u32;
-            bad |= valid && !ins && !okg;
-            const float *src = ins ? sHi + loc : (okg ? A.uhi_in + idx : hi + fm[p]);
-            v = *src;
-          }
-          fl[ff][p] = v;
-        }
-      }
-      if (bad) atomicExch(A.status, kStatusBadGather);
-    }
-
-    // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into three BF16 parts ----
-    const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
-    const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
-    const double wA = cons ? 0.5 * uA * uA : uA;
-    const double dB = (cons ? 0.5 * uB * uB : uB) - wA;
-    const double dC = (cons ? 0.5 * uC * uC : uC) - wA;
-    const double dD = (cons ? 0.5 * uD * uD : uD) - wA;
-    const float L0 = (float)(0.5 * ((double)cr * dB + (double)cs * dC + (double)ct * dD));
-    if (got && valid) {
-#pragma unroll
-      for (int c = h; c < KV / 8; c += TPE) {
-        float v[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int j = 8 * c + q;
-          v[q] = 0.f;
-          if (j < NP) {
-            const double uj = (double)hi[j] + (double)lo[j];
-            const double wj = cons ? 0.5 * uj * uj : uj;
-            v[q] = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
+          for (int p = 0; p < KF; ++p) {
+            float v = 0.f;
+            if (p < NFP && got) {
+              const uint32_t idx = nb + ((rw[p >> 2] >> (8 * (p & 3))) & 0xffu);
+              const uint32_t loc = idx - (uint32_t)slot0;
+              const bool ins = loc < (uint32_t)slotn;
+              const bool okg = idx < n_u32;
+              bad |= valid && !ins && !okg;
+              const float *src = ins ? sHi + loc : (okg ? A.uhi_in + idx : hi + fm[p]);
+              v = *src;
+            }
+            fl[ff][p] = v;
           }
         }
-        store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, v);
+        if (bad) atomicExch(A.status, kStatusBadGather);
       }
-    }
-    fence_async_smem();  // the A buffer is read by the tensor cores (async proxy)
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    mbar_arrive(avol);
-    if (!got || vload(&sMisc[0])) {
-      failed = true;
-      break;
-    }
 
-    // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
+      // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into three BF16 parts ----
+      const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
+      const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
+      const double wA = cons ? 0.5 * uA * uA : uA;
+      const double dB = (cons ? 0.5 * uB * uB : uB) - wA;
+      const double dC = (cons ? 0.5 * uC * uC : uC) - wA;
+      const double dD = (cons ? 0.5 * uD * uD : uD) - wA;
+      const float L0 = (float)(0.5 * ((double)cr * dB + (double)cs * dC + (double)ct * dD));
+      if (got && valid) {
 #pragma unroll
-    for (int ff = 0; ff < FPT; ++ff) {
-      const int f = h * FPT + ff;
-      const float g = f == 0 ? g0.w : f == 1 ? g1.x : f == 2 ? g1.y : g1.z, ga = fabsf(g);
-      const uint8_t *fm = sFm + f * NFP;
-#pragma unroll
-      for (int p = 0; p < NFP; ++p) {
-        const float uM = hi[fm[p]], uP = fl[ff][p];
-        const float d = uM - uP;
-        fl[ff][p] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
-      }
-    }
-
-    // the volume MMAs have read the A buffer (and written acc_V) once mvol completes
-    const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (vdone && valid) {
-#pragma unroll
-      for (int ff = 0; ff < FPT; ++ff) {
-        const int f = h * FPT + ff;
-#pragma unroll
-        for (int cq = 0; cq < KF / 8; ++cq) {
+        for (int c = h; c < KV / 8; c += TPE) {
           float v[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) v[q] = fl[ff][8 * cq + q];
-          store_split8(sA + (size_t)kmaj(e, f * KF + 8 * cq, TE) * 2, C::A_PART, v);
+          for (int q = 0; q < 8; ++q) {
+            const int j = 8 * c + q;
+            v[q] = 0.f;
+            if (j < NP) {
+              const double uj = (double)hi[j] + (double)lo[j];
+              const double wj = cons ? 0.5 * uj * uj : uj;
+              v[q] = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
+            }
+          }
+          store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, v);
         }
       }
-    }
-    fence_async_smem();
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    mbar_arrive(alift);
-    if (!vdone) {
-      failed = true;
-      break;
-    }
+      fence_async_smem();  // the A buffer is read by the tensor cores (async proxy)
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(avol);
+      if (!got || vload(&sMisc[0])) {
+        failed = true;
+        break;
+      }
 
-    // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
-    constexpr int NCE = ((NP + 7) / 8 + TPE - 1) / TPE;  // epilogue chunks per thread
-    float t0[NCE][8];
+      // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
 #pragma unroll
-    for (int cc = 0; cc < NCE; ++cc) {
-      const int c = h + TPE * cc;
-      if (c < (NP + 7) / 8) {
-        float dv[24];  // columns 3i+d of nodes 8c..8c+7
-        tmem_ld24(lane_tmem + 24 * c, dv);
+      for (int ff = 0; ff < FPT; ++ff) {
+        const int f = h * FPT + ff;
+        const float g = f == 0 ? g0.w : f == 1 ? g1.x : f == 2 ? g1.y : g1.z, ga = fabsf(g);
+        const uint8_t *fm = sFm + f * NFP;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int i = min(8 * c + q, NP - 1);
-          const float dd = fmaf(cr, dv[3 * q], fmaf(cs, dv[3 * q + 1], fmaf(ct, dv[3 * q + 2], L0)));
-          const float vol = cons ? -dd : -hi[i] * dd;
-          t0[cc][q] = fmaf(a, sRe[ee * NP + i], dt * vol);
+        for (int p = 0; p < NFP; ++p) {
+          const float uM = hi[fm[p]], uP = fl[ff][p];
+          const float d = uM - uP;
+          fl[ff][p] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
         }
       }
-    }
 
-    // ---- LIFT accumulator and the compensated stage update into the slot ----
-    const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
-    if (ldone) {
+      // the volume MMAs have read the A buffer (and written acc_V) once mvol completes
+      const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (vdone && valid) {
+#pragma unroll
+        for (int ff = 0; ff < FPT; ++ff) {
+          const int f = h * FPT + ff;
+#pragma unroll
+          for (int cq = 0; cq < KF / 8; ++cq) {
+            float v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = fl[ff][8 * cq + q];
+            store_split8(sA + (size_t)kmaj(e, f * KF + 8 * cq, TE) * 2, C::A_PART, v);
+          }
+        }
+      }
+      fence_async_smem();
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      mbar_arrive(alift);
+      if (!vdone) {
+        failed = true;
+        break;
+      }
+
+      // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
+      constexpr int NCE = ((NP + 7) / 8 + TPE - 1) / TPE;  // epilogue chunks per thread
+      float t0[NCE][8];
 #pragma unroll
       for (int cc = 0; cc < NCE; ++cc) {
         const int c = h + TPE * cc;
         if (c < (NP + 7) / 8) {
-          float lf[8];
-          tmem_ld8(lane_tmem + NV + 8 * c, lf);
+          float dv[24];  // columns 3i+d of nodes 8c..8c+7
+          tmem_ld24(lane_tmem + 24 * c, dv);
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
-            const int i = 8 * c + q;
-            if (i < NP && valid) {
-              const int o = e * NP + i;
-              const float rn = fmaf(dt, lf[q], t0[cc][q]);
-              float hn, ln;
-              stage_update(hi[i], lo[i], rn, bh, bl, hn, ln);
-              sHi[o] = hn;
-              sLo[o] = ln;
-              sRe[o] = rn;
-              if ((uint32_t)o >= tail0) {
-                A.uhi_out[slot0 + o] = hn;
-                A.ulo_out[slot0 + o] = ln;
-                A.resu[slot0 + o] = rn;
+            const int i = min(8 * c + q, NP - 1);
+            const float dd = fmaf(cr, dv[3 * q], fmaf(cs, dv[3 * q + 1], fmaf(ct, dv[3 * q + 2], L0)));
+            const float vol = cons ? -dd : -hi[i] * dd;
+            t0[cc][q] = fmaf(a, sRe[ee * NP + i], dt * vol);
+          }
+        }
+      }
+
+      // ---- LIFT accumulator and the compensated stage update into the slot ----
+      const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
+      if (ldone) {
+#pragma unroll
+        for (int cc = 0; cc < NCE; ++cc) {
+          const int c = h + TPE * cc;
+          if (c < (NP + 7) / 8) {
+            float lf[8];
+            tmem_ld8(lane_tmem + NV + 8 * c, lf);
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+              const int i = 8 * c + q;
+              if (i < NP && valid) {
+                const int o = e * NP + i;
+                const float rn = fmaf(dt, lf[q], t0[cc][q]);
+                float hn, ln;
+                stage_update(hi[i], lo[i], rn, bh, bl, hn, ln);
+                sHi[o] = hn;
+                sLo[o] = ln;
+                sRe[o] = rn;
+                if ((uint32_t)o >= tail0) {
+                  A.uhi_out[slot0 + o] = hn;
+                  A.ulo_out[slot0 + o] = ln;
+                  A.resu[slot0 + o] = rn;
+                }
               }
             }
           }
         }
       }
+      if (!ldone) {
+        failed = true;
+        break;
+      }
+      fence_async_smem();  // the slot writes become visible to the producer's bulk stores
+      mbar_arrive(&done[s]);
     }
-    if (!ldone) {
-      failed = true;
-      break;
+    if (failed && lane == 0) {
+      atomicExch(A.status, kStatusTimeoutCode);
+      *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
     }
-    fence_async_smem();  // the slot writes become visible to the producer's bulk stores
-    mbar_arrive(&done[s]);
-  }
-  if (failed && lane == 0) {
-    atomicExch(A.status, kStatusTimeoutCode);
-    *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
-  }
   }  // consumers
   // consumers and the MMA warp: TMEM is freed once every load from it and every MMA into it is done
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -565,7 +563,8 @@ void prepare_tcm_cw(int cw) {
 template <int N>
 bool launch_tcm_cw(const MixedArgs &A, int cw, int num_sms, cudaStream_t st, LaunchInfo *info) {
   const bool cons = A.conservative != 0;
-  if (cw == 8) return cons ? launch_tcm_n<N, 8, true>(A, num_sms, st, info) : launch_tcm_n<N, 8, false>(A, num_sms, st, info);
+  if (cw == 8)
+    return cons ? launch_tcm_n<N, 8, true>(A, num_sms, st, info) : launch_tcm_n<N, 8, false>(A, num_sms, st, info);
   if (cw == 16)
     return cons ? launch_tcm_n<N, 16, true>(A, num_sms, st, info) : launch_tcm_n<N, 16, false>(A, num_sms, st, info);
   return false;
