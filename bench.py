@@ -61,16 +61,38 @@ def b_alg_per_dof(N: int, elem_bytes: int) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 100 ms while running."""
+    """SM clocks and throttle reasons sampled while running: NVML reads every 2 ms from a thread (short timed
+    regions still get samples), else nvidia-smi every 100 ms."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index: int):
-        self.index, self.rows, self.proc = index, [], None
+    def __init__(self, index: int, period_s: float = 0.002):
+        self.index, self.period, self.rows, self.proc, self.nv = index, period_s, [], None, None
+        self.stop = threading.Event()
+
+    def _nvml_index(self):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v for v in vis.split(",") if v.strip()]
+        if ids and all(v.strip().isdigit() for v in ids) and self.index < len(ids):
+            return int(ids[self.index])
+        return self.index
 
     def __enter__(self):
+        try:
+            import pynvml as nv
+            nv.nvmlInit()
+            self.nv, self.h = nv, nv.nvmlDeviceGetHandleByIndex(self._nvml_index())
+            self.masks = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                          nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM)
+            self.t = threading.Thread(target=self._poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -81,11 +103,30 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv = self.nv
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.rows.append([str(self.index), str(sm), str(self.smax), "", ""] +
+                                 ["Active" if rs & m else "Not Active" for m in self.masks])
+            except Exception:
+                return
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
             self.rows.append([c.strip() for c in line.split(",")])
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nv is not None:
+            self.t.join(timeout=1)
+            try:
+                self.nv.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -98,10 +139,10 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
         sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        reasons = sorted({self.NAMES[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml" if self.nv else "nvidia-smi"}
 
 
 def dist_setup(args):
@@ -150,14 +191,18 @@ def time_stages(prob, steps: int, stream):
     return e0.elapsed_time(e1) / steps  # ms per stage
 
 
-def cpu_baseline(N: int, steps: int, seconds: float = 12.0, n: int = 16):
-    """Oracle port (C restatement of the OKL loops, OpenMP over the @outer partition loop) on a bounded
-    sample of the same workload: order N, 16 x-slab partitions of an n^3 x 6 Kuhn mesh (n = 16: 24,576 tets),
-    set up by the oracle's own numpy restatement of the reference's setup chain (no GPU involved)."""
+def cpu_baseline(N: int, steps: int, seconds: float = 12.0, n: int = 16, slabs: int = 16, serial_stages: int = 0):
+    """Oracle port (C restatement of the OKL loops, OpenMP over the @outer partition loop) on the host cores:
+    order N, `slabs` x-slab partitions of an n^3 x 6 Kuhn mesh, set up by the oracle's own numpy restatement of
+    the reference's setup chain (no GPU involved).  Times `steps` stages (or as many as fit in `seconds` when
+    steps is 0) with one thread per partition up to the host's cores, then `serial_stages` stages on 1 thread
+    (the OCCA Serial mode)."""
     from oracle import burgers_ref as BR
     from oracle import oracle as O
-    ref = BR.Problem(N, n, 16, "modes")
+    t0 = time.perf_counter()
+    ref = BR.Problem(N, n, slabs, "modes")
     rs = O.RunState(ref)
+    setup_s = time.perf_counter() - t0
     u = np.ascontiguousarray(ref.u0, dtype=np.float64).copy()
     resu = np.zeros_like(u)
     P = len(rs.K)
@@ -171,22 +216,35 @@ def cpu_baseline(N: int, steps: int, seconds: float = 12.0, n: int = 16):
         if (steps and done >= steps) or (not steps and el_t >= seconds):
             break
     value = u.size * done / el_t
-    return {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"order {N}, {n}^3x6 Kuhn mesh ({ref.K:,} tets, {P} x-slab partitions), {done} LSERK4 stages of "
-                      f"exchange + LF RHS + update, C restatement of the OKL loops (gcc -O3 -fopenmp, "
-                      f"-ffp-contract=off), OpenMP over partitions, {threads} threads of {os.cpu_count()} host cores",
-            "seconds": el_t}
+    out = {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+           "sample": f"order {N}, {n}^3x6 Kuhn mesh ({ref.K:,} tets, {P} x-slab partitions), {done} LSERK4 stages of "
+                     f"exchange + LF RHS + update, C restatement of the OKL loops (gcc -O3 -fopenmp, "
+                     f"-ffp-contract=off), OpenMP over partitions, {threads} threads of {os.cpu_count()} host cores",
+           "seconds": el_t, "setup_s": setup_s}
+    if serial_stages:
+        t0 = time.perf_counter()
+        rs.run(u, resu, ref.dt, serial_stages, done % 5, 0, 1)
+        ser = time.perf_counter() - t0
+        out["serial"] = {"value": u.size * serial_stages / ser, "unit": UNIT, "cores": 1, "stages": serial_stages,
+                         "seconds": ser}
+    return out
 
 
 def run_reference(args, world, rank):
+    """The reference arm: the oracle port of the reference's OKL loops on the host cores, on the same workload as
+    our arm (order, mesh, partitions, u0), `steps` stages after one warm-up stage; plus a Serial (1 core)
+    sample."""
     if rank != 0:
         return
-    base = cpu_baseline(args.order, args.steps)
+    base = cpu_baseline(args.order, args.steps, n=args.n, slabs=args.slabs, serial_stages=1)
+    Np = (args.order + 1) * (args.order + 2) * (args.order + 3) // 6
     out = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": base["seconds"] / max(1, args.steps) * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": f"3-D Burgers tet-DG LSERK4 stage, order {args.order}, sampled on a 16^3x6 "
-                                  f"periodic Kuhn mesh with 16 x-slab partitions (the reference's CPU path)"},
+           "config": {"workload": f"3-D Burgers tet-DG, order {args.order} (Np={Np}), periodic {args.n}^3x6 Kuhn "
+                                  f"mesh (K={6 * args.n ** 3}), {args.slabs} x-slab partitions, u0 = 0.5 + 8 seeded "
+                                  f"Fourier modes; one step = one LSERK4 stage (the reference's CPU path: OpenMP "
+                                  f"over partitions, one warm-up stage; Serial 1-core sample in cpu_baseline.serial)"},
            "cpu_baseline": base, "e2e": {"value": base["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                          "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -376,7 +434,7 @@ def main():
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=64)
+    ap.add_argument("--n", "--cubes", dest="n", type=int, default=64, help="cubes per axis of the Kuhn mesh")
     ap.add_argument("--order", type=int, default=4)
     ap.add_argument("--slabs", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=8)
@@ -403,6 +461,38 @@ def main():
             dist.destroy_process_group()
 
 
+def volume_microbench(prob, stream, hbm, local, launches: int = 20, warmup: int = 3):
+    """The standalone volume derivative (`differentiate`: Dr/Ds/Dt applied to u, then the nine per-node metrics)
+    on the benchmark mesh, FP64, in HBM GB/s by the reference's own formula 13 * 8 B * Np * K / t (U, nine
+    metrics, three outputs; tetnudg/tet_nudg_mesh_physical_derivative_test.go:544-547).  Every launch streams
+    13 arrays of K Np doubles, far larger than L2.  Checked against the analytic derivative of the initial
+    field (a size-independent property: the interpolation error of the order-N nodal field)."""
+    import torch
+    from dgkernel_b200.burgers import random_modes, DEFAULT_SEED
+    prob.differentiate(warmup)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        prob.differentiate(launches)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / launches
+    Np, K = prob.el.Np, prob.K
+    nbytes = 13 * 8 * Np * K
+    gbs = nbytes / (ms * 1e-3) / 1e9
+    X, Y, Z = prob.get("X"), prob.get("Y"), prob.get("Z")
+    ux = np.zeros_like(X)
+    for kx, ky, kz, a, phi in random_modes(DEFAULT_SEED):
+        ux -= a * np.pi * kx * np.sin(np.pi * (kx * X + ky * Y + kz * Z) + phi)
+    got = prob.get("DuDx")
+    err = float(np.linalg.norm(got - ux) / np.linalg.norm(ux))
+    return {"value": gbs, "unit": "GB/s", "ms_per_launch": ms, "launches": launches, "bytes_per_launch": nbytes,
+            "formula": "13 * 8 B * Np * K / t (tet_nudg_mesh_physical_derivative_test.go:544-547)",
+            "hbm_frac": gbs / hbm, "dof_per_s": Np * K / (ms * 1e-3), "kernel": "diff_kernel",
+            "dudx_rel_err_vs_analytic": err, "clocks": clk.summary()}
+
+
 def run_burgers(args, world, rank, local):
     """The default line (order 4, 64^3 x 6): plain FP64, plain FP32 and the mixed forms from one u0; the chosen
     form."""
@@ -419,8 +509,13 @@ def run_burgers(args, world, rank, local):
         forms.append(("mixed_tc", MIXED, {"mma": True}))
     kernels = {"f64": "rhs_stage_dmma_kernel", "f32": "rhs_stage_kernel", "mixed": "rhs_stage_mixed_kernel",
                "mixed_tc": "rhs_stage_tcm_kernel"}
+    micro = None
     for name, dt, kw in forms:
+        if name == "f64":
+            kw = dict(kw, derivatives=True)
         prob = BurgersProblem(args.order, args.n, args.slabs, dt, "modes", stream=stream.cuda_stream, **kw)
+        if name == "f64":
+            micro = volume_microbench(prob, stream, hbm, local)
         prob.run_stages(args.warmup)
         barrier(world)
         with ClockSampler(local) as clk:
@@ -512,6 +607,7 @@ def run_burgers(args, world, rank, local):
             "plain_fp64_roofline": {"bound": "hbm", "achieved": plain_ach, "peak": hbm, "unit": "GB/s",
                                     "frac": plain_ach / hbm, "b_alg_per_dof": f64["b_alg"],
                                     "kernel": f64["kernel"]},
+            "microbench": micro,
             "cpu_baseline": cpu,
             "e2e": {"value": world * dofs / e2e_s, "unit": UNIT, "h2d_bytes_per_step": e2e_bytes,
                     "d2h_bytes_per_step": e2e_bytes,

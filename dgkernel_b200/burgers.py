@@ -34,6 +34,7 @@ RK4B = (1432997174477.0 / 9575080441755.0, 5161836677717.0 / 13612068292357.0,
 DEFAULT_SEED = 20261203
 GEO = ("Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz")
 FACE = ("nx", "ny", "nz", "Fscale")
+DERIV = ("DuDx", "DuDy", "DuDz")
 
 
 class UniformStream:
@@ -134,6 +135,9 @@ class _TetBurgers:
         params = [Temp(nm).Type(dt_code).Size(K * Np) for nm in state + GEO]
         params += [Temp(nm).Type(dt_code).Size(K * NF) for nm in FACE]
         params += [Temp("gmap").Type(INT32).Size(K * NF), Temp("vmapP").Type(INT64).Size(K * NF)]
+        if getattr(self, "derivatives", False):
+            # outputs of the standalone volume-derivative operator (`differentiate`) on this mesh
+            params += [Temp(nm).Type(dt_code).Size(K * Np) for nm in DERIV]
         if self.mixed:
             # 128-byte partition starts: the mixed stage streams each partition's slots with 16-byte bulk copies
             params += [Temp(nm).Type(Float32).Size(K * Np).Align(WarpAlign)
@@ -272,6 +276,19 @@ class _TetBurgers:
         if self.mixed and name == "u":
             self.runner.ExecuteKernel("splitState")
 
+    def differentiate(self, repeats: int = 1):
+        """DuDx, DuDy, DuDz of the current u through the `differentiate` operator (Dr/Ds/Dt then the nine
+        per-node metrics; tetnudg/tet_nudg_mesh_physical_derivative_test.go:921-1078), `repeats` launches."""
+        if not getattr(self, "derivatives", False) or self.mixed:
+            raise ValueError("problem built without derivative outputs (derivatives=True, float dtype)")
+        r, sn = self.runner, self.el.ShortName
+        if "differentiate" not in r.KernelConfigs:
+            r.ConfigureKernel("differentiate", r.Param("u"), *[r.Param(n) for n in GEO],
+                              *[r.Param(n) for n in DERIV], *[r.Param(f"{m}_{sn}") for m in ("Dr", "Ds", "Dt")])
+            r.BuildKernel("differentiate", "differentiate")
+        for _ in range(repeats):
+            r.ExecuteKernel("differentiate")
+
     def run_stages(self, nstages: int):
         """Advance by nstages LSERK4 stages (stage index continues across calls)."""
         for _ in range(nstages):
@@ -304,8 +321,9 @@ class BurgersProblem(_TetBurgers):
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
                  cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None,
                  viscosity=None, eps0: float = 1.0, c0: float = 0.0, kappa: float = 1.0, conf=(0.1, 0.9),
-                 mode_sigma: float = 0.1, tensor=None, mma=None):
+                 mode_sigma: float = 0.1, tensor=None, mma=None, derivatives=False):
         self.n, self.nslab = n, nslab
+        self.derivatives = derivatives  # also bind DuDx, DuDy, DuDz for the `differentiate` operator
         self.tensor = tensor  # mixed form: None = by order (tensor cores for orders 6, 7), True / False to force
         self.mma = mma  # mixed form, orders 1..4: element-local products on the tensor cores (3-part BF16)
         VX, VY, VZ, EToV, EToVp, EToP = M.kuhn_mesh(n, nslab)

@@ -52,12 +52,14 @@ extern "C" int dgk_convert_upload_noalloc(const void *host, int32_t host_dtype, 
   try {
     if (count < 0 || (count > 0 && (!host || !device_dst)))
       throw dgk::Error(DGK_ERR_INVALID, "null buffer or negative count");
-    const size_t bytes = (size_t)count * (size_t)dgk::dtype_size(host_dtype);
+    const size_t esize = (size_t)dgk::dtype_size(host_dtype);
     dgk::dtype_size(dev_dtype);
-    if (bytes > kNoAllocScratchBytes)
-      throw dgk::Error(DGK_ERR_INVALID, "dgk_convert_upload_noalloc: " + std::to_string(bytes) +
-                                            " bytes of host data exceed the fixed 8 MiB staging area; split the "
+    // compare counts, not byte products: count * esize could wrap around for a huge count
+    if ((uint64_t)count > kNoAllocScratchBytes / esize)
+      throw dgk::Error(DGK_ERR_INVALID, "dgk_convert_upload_noalloc: " + std::to_string(count) +
+                                            " host values exceed the fixed 8 MiB staging area; split the "
                                             "upload into calls of at most 8 MiB of host data");
+    const size_t bytes = (size_t)count * esize;
     if (count == 0) return DGK_OK;
     void *scratch = scratch_address();  // first call on a device resolves the address (do it before a capture)
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);

@@ -112,8 +112,26 @@ def u0_modes(X, Y, Z, modes, mean: float = 0.5):
     return u
 
 
-def h_min(X, Y, Z) -> float:
-    """Smallest node-pair distance > 1e-12 over all elements (3d_scalar_burgers_equation.go:697-717)."""
+def h_min(X, Y, Z, chunk=8192) -> float:
+    """Smallest node-pair distance > 1e-12 over all elements (3d_scalar_burgers_equation.go:697-717), in chunks
+    of elements; the same distances as the per-element loop (h_min_loop), so the same minimum."""
+    K, Np = X.shape
+    iu = np.triu_indices(Np, 1)
+
+    def one(c0):
+        x, y, z = X[c0:c0 + chunk], Y[c0:c0 + chunk], Z[c0:c0 + chunk]
+        dx = x[:, :, None] - x[:, None, :]
+        dy = y[:, :, None] - y[:, None, :]
+        dz = z[:, :, None] - z[:, None, :]
+        d = np.sqrt(dx * dx + dy * dy + dz * dz)[:, iu[0], iu[1]]
+        d = d[d > 1e-12]
+        return float(d.min()) if d.size else math.inf
+
+    return min(g.parallel_chunks(one, K, chunk), default=math.inf)
+
+
+def h_min_loop(X, Y, Z) -> float:
+    """Per-element loop form of h_min (checks the chunked form)."""
     best = math.inf
     for k in range(X.shape[0]):
         p = np.stack((X[k], Y[k], Z[k]), axis=1)

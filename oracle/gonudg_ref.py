@@ -17,6 +17,8 @@ Deliberate restatements of reference quirks (parity is to the reference, not to 
 from __future__ import annotations
 
 import math
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -470,12 +472,63 @@ def ti_connect3d(EToV):
     return EToE, EToF
 
 
-def build_maps3d(el: RefElement, X, Y, Z, EToE, EToF, period=None):
-    """VmapM/VmapP/MapP by nearest face node within NODETOL (buildmaps3d.go:5-153).
+def build_maps3d(el: RefElement, X, Y, Z, EToE, EToF, period=None, chunk=65536):
+    """VmapM/VmapP/MapP by nearest face node within NODETOL (buildmaps3d.go:5-153), all face pairs at once in
+    chunks of `chunk` faces.  Same arithmetic and the same first-minimum choice as the per-face loop
+    (build_maps3d_loop, the line-by-line restatement), so the results are identical; this form scales to the
+    benchmark meshes.
 
     ``period`` (a length-3 sequence or None) is this build's periodic extension: coordinate
     differences are wrapped into [-L/2, L/2] before the same NODETOL^2 distance test.
     """
+    K, Np, Nfp = X.shape[0], el.Np, el.Nfp
+    NF = Nfp * NFACES
+    fm = el.Fmask.reshape(-1)
+    vmapM = (fm[None, :] + (np.arange(K) * Np)[:, None]).reshape(-1)
+    vmapP = vmapM.copy()
+    mapP = np.arange(K * NF)
+    x, y, z = X.reshape(-1), Y.reshape(-1), Z.reshape(-1)
+    EToE = np.asarray(EToE, dtype=np.int64).reshape(-1)
+    EToF = np.asarray(EToF, dtype=np.int64).reshape(-1)
+    faces = np.arange(K * NFACES)
+    k1, f1 = faces // NFACES, faces % NFACES
+    conn = np.nonzero(~((EToE == k1) & (EToF == f1)))[0]  # faces with a neighbour (the loop skips the others)
+    pts = np.arange(Nfp)
+
+    def one(c0):
+        fc = conn[c0:c0 + chunk]
+        idsM = (fc // NFACES)[:, None] * NF + (fc % NFACES)[:, None] * Nfp + pts[None, :]
+        idsP = EToE[fc][:, None] * NF + EToF[fc][:, None] * Nfp + pts[None, :]
+        vidM, vidP = vmapM[idsM], vmapM[idsP]
+        dx = x[vidP][:, None, :] - x[vidM][:, :, None]
+        dy = y[vidP][:, None, :] - y[vidM][:, :, None]
+        dz = z[vidP][:, None, :] - z[vidM][:, :, None]
+        if period is not None:
+            dx = _wrap(dx, period[0])
+            dy = _wrap(dy, period[1])
+            dz = _wrap(dz, period[2])
+        D = dx * dx + dy * dy + dz * dz
+        jmin = np.argmin(D, axis=2)
+        ok = np.take_along_axis(D, jmin[..., None], axis=2)[..., 0] < NODETOL * NODETOL
+        vmapP[idsM[ok]] = np.take_along_axis(vidP, jmin, axis=1)[ok]  # chunks write disjoint entries
+        mapP[idsM[ok]] = np.take_along_axis(idsP, jmin, axis=1)[ok]
+
+    parallel_chunks(one, len(conn), chunk)
+    mapB = np.nonzero(mapP == np.arange(K * NF))[0]
+    return vmapM, vmapP, mapP, mapB
+
+
+def parallel_chunks(fn, n, chunk):
+    """fn(c0) for c0 = 0, chunk, 2 chunk, ... < n on a thread pool (numpy releases the GIL in its kernels)."""
+    starts = list(range(0, n, chunk))
+    if len(starts) <= 1:
+        return [fn(c0) for c0 in starts]
+    with ThreadPoolExecutor(max_workers=min(len(starts), os.cpu_count() or 1)) as ex:
+        return list(ex.map(fn, starts))
+
+
+def build_maps3d_loop(el: RefElement, X, Y, Z, EToE, EToF, period=None):
+    """Per-face loop form of build_maps3d, line by line after buildmaps3d.go:46-153 (checks the batched form)."""
     K, Np, Nfp = X.shape[0], el.Np, el.Nfp
     NF = Nfp * NFACES
     fm = el.Fmask.reshape(-1)
@@ -508,8 +561,11 @@ def build_maps3d(el: RefElement, X, Y, Z, EToE, EToF, period=None):
 
 
 def _wrap(d, L):
-    d = np.where(d > 0.5 * L, d - L, d)
-    return np.where(d < -0.5 * L, d + L, d)
+    """d - L where d > L/2, d + L where d < -L/2 (in place on a float array)."""
+    d = np.array(d, dtype=np.float64, copy=True)
+    np.subtract(d, L, out=d, where=d > 0.5 * L)
+    np.add(d, L, out=d, where=d < -0.5 * L)
+    return d
 
 
 # --------------------------------------------------------------------------------------------------
@@ -525,7 +581,40 @@ class FaceConnector:
 
 
 def face_connector(K: int, Nfaces: int, Nfp: int, Np: int, vmapP, EToP) -> FaceConnector:
-    """NewFaceConnector + BuildIndices (face_connector.go:43-187)."""
+    """NewFaceConnector + BuildIndices (face_connector.go:43-187), one partition at a time: the destination
+    partition's face points in (local element, point) order, split by source partition with a stable mask.
+    That is the order in which the reference's per-element loop appends (face_connector_loop restates that
+    loop), so the lists are identical."""
+    vmapP = np.asarray(vmapP, dtype=np.int64)
+    EToP = np.asarray(EToP, dtype=np.int64)
+    if K <= 0 or Nfaces <= 0 or Nfp <= 0 or Np <= 0:
+        raise ValueError("invalid dimensions")
+    if len(vmapP) != K * Nfaces * Nfp or len(EToP) != K:
+        raise ValueError("length mismatch")
+    P = int(EToP.max()) + 1
+    l2g = [np.nonzero(EToP == p)[0] for p in range(P)]
+    g2l = np.zeros(K, dtype=np.int64)
+    for p in range(P):
+        g2l[l2g[p]] = np.arange(len(l2g[p]))
+    NF = Nfaces * Nfp
+    pick = [[None] * P for _ in range(P)]
+    place = [[None] * P for _ in range(P)]
+    for p in range(P):
+        src = vmapP[(l2g[p][:, None] * NF + np.arange(NF)[None, :]).reshape(-1)]
+        se = src // Np
+        sp = EToP[se]
+        lsrc = g2l[se] * Np + src % Np
+        for q in range(P):
+            sel = np.nonzero(sp == q)[0]
+            pick[q][p] = lsrc[sel].astype(np.int64)
+            place[p][q] = sel.astype(np.int64)  # = local element * NF + face point
+    fc = FaceConnector(P, [len(v) for v in l2g], l2g)
+    fc.pick, fc.place = pick, place
+    return fc
+
+
+def face_connector_loop(K: int, Nfaces: int, Nfp: int, Np: int, vmapP, EToP) -> FaceConnector:
+    """Per-element loop form of face_connector after face_connector.go:143-187 (checks the batched form)."""
     vmapP = np.asarray(vmapP, dtype=np.int64)
     EToP = np.asarray(EToP, dtype=np.int64)
     if K <= 0 or Nfaces <= 0 or Nfp <= 0 or Np <= 0:

@@ -1,7 +1,7 @@
 """Extract the reference's own golden vectors and in-code test meshes into tests/golden/reference_golden.json.
 
-Run once in a checkout that has the DGKernel sources (default /root/reference, or DGK_REFERENCE_ROOT); the
-JSON it writes is committed, so the tests never read the reference at run time.  It reads the reference's
+Run once in a checkout that has the DGKernel sources: pass the project root as the first argument or in
+DGK_REFERENCE_ROOT (`python tests/golden/make_golden.py <DGKernel root>`); the JSON it writes is committed, so the tests never read the reference at run time.  It reads the reference's
 Go test files as text:
 
   * element/library/gonudg/jacobi_quadrature_test.go  TestJacobiGL table (alpha, beta, N, expected nodes)
@@ -16,7 +16,7 @@ import os
 import re
 import sys
 
-ROOT = os.environ.get("DGK_REFERENCE_ROOT", "/root/reference")
+ROOT = ""
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
 
 
@@ -66,6 +66,11 @@ def meshes(text: str):
 
 
 def main():
+    global ROOT
+    ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DGK_REFERENCE_ROOT", "")
+    if not ROOT or not os.path.isdir(ROOT):
+        sys.stderr.write("usage: make_golden.py <DGKernel root>  (or set DGK_REFERENCE_ROOT)\n")
+        return 2
     g = os.path.join(ROOT, "element", "library", "gonudg")
     with open(os.path.join(g, "jacobi_quadrature_test.go")) as f:
         quad = f.read()

@@ -43,11 +43,14 @@ def test_rank_setup_barrier_and_max_over_ranks(tmp_path):
 
 
 def test_reference_arm_two_ranks_prints_once():
-    r = _torchrun("bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--order", "2")
+    r = _torchrun("bench.py", "--impl", "reference", "--gpus", "2", "--steps", "1", "--warmup", "3", "--order", "2",
+                  "--cubes", "8", "--slabs", "4")
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["cores"] >= 1
+    assert d["cpu_baseline"]["serial"]["cores"] == 1 and d["cpu_baseline"]["serial"]["value"] > 0
+    assert "8^3x6" in d["config"]["workload"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}

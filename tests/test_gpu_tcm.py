@@ -81,3 +81,24 @@ def test_tcm_stage_matches_three_part_restatement():
     print(f"tensor-core mixed stage vs three-part restatement: {err:.3e}")
     assert err < 3e-6, err
     P.free()
+
+
+@pytest.mark.parametrize("form", ["fp64", "mixed_tc"])
+def test_benchmark_shaped_mesh_pinned_to_oracle(form):
+    """The benchmark's shape at a size the oracle runs in seconds: order 4, 16 x-slab partitions of a 16^3 x 6
+    mesh (24,576 tets, 192 tensor-core tiles), the random-mode u0 of the benchmark, 10 LSERK4 stages through
+    the runner, against the oracle's own setup and run: plain FP64 stage <= 1e-12, tensor-core mixed stage
+    <= MMA_TOL."""
+    kw = {"mma": True} if form == "mixed_tc" else {}
+    P = BurgersProblem(4, 16, 16, MIXED if form == "mixed_tc" else np.float64, "modes", **kw)
+    ref = b.Problem(4, 16, 16, "modes")
+    assert rel_l2(P.u0, ref.u0) < 1e-15
+    rs = O.RunState(ref)
+    u = np.ascontiguousarray(ref.u0, dtype=np.float64).copy()
+    resu = np.zeros_like(u)
+    rs.run(u, resu, P.dt, 10, threads=8)
+    P.run_stages(10)
+    err = rel_l2(P.get("u"), u)
+    print(f"{form}: relative L2 vs oracle after 10 stages at 16^3 x 6, 16 slabs: {err:.3e}")
+    assert err < (1e-12 if form == "fp64" else MMA_TOL), err
+    P.free()

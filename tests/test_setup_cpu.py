@@ -89,3 +89,20 @@ def test_splitmix_stream_and_modes_match_oracle():
     pm = random_modes(b.DEFAULT_SEED)
     for row, (k, a, phi) in zip(pm, om):
         assert list(row[:3]) == k and row[3] == a and row[4] == phi
+
+
+def test_oracle_batched_setup_equals_its_loop_restatement():
+    """The oracle's batched BuildMaps3D, FaceConnector and h_min (used at the benchmark's mesh size) give
+    exactly the lists and values of their per-face / per-element loop restatements."""
+    from oracle import burgers_ref as br
+    for N, n, P in ((2, 4, 2), (3, 5, 5)):
+        p = br.Problem(N, n, P, "modes")
+        loop = g.build_maps3d_loop(p.el, p.X, p.Y, p.Z, p.EToE, p.EToF, period=(2.0, 2.0, 2.0))
+        for x, y in zip(loop, (p.vmapM, p.vmapP, p.mapP, p.mapB)):
+            assert np.array_equal(x, y)
+        fl = g.face_connector_loop(p.K, 4, p.el.Nfp, p.el.Np, p.vmapP, p.EToP)
+        for a in range(P):
+            for b in range(P):
+                assert np.array_equal(fl.pick[a][b], p.fc.pick[a][b])
+                assert np.array_equal(fl.place[a][b], p.fc.place[a][b])
+        assert br.h_min_loop(p.X, p.Y, p.Z) == p.hmin

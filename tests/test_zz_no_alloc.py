@@ -6,7 +6,8 @@ budget, or a time-stepping loop that cannot absorb a cudaMalloc -- use the alloc
 stages through a fixed 8 MiB array in the library's device image.  The two paths must write identical device
 data (the conversion is exact, so the tolerance is zero), on two calls in a row, and sizes beyond the fixed
 array must be refused.  This file is collected last so that a stop-at-first-failure run has run every other
-test before it.
+test before it.  The refusal of an oversized count happens before any device work, so it is also checked
+without a GPU.
 """
 import ctypes
 
@@ -17,9 +18,18 @@ import dgkernel_b200 as d
 from dgkernel_b200 import _lib
 from dgkernel_b200.runner import Config, Float32, Input, Runner
 
-pytestmark = pytest.mark.gpu
+
+def test_noalloc_refuses_wrapping_count_without_device_work():
+    # count * 8 wraps to 0 in 64 bits; the size check must refuse it before any copy or launch
+    L = _lib.lib()
+    buf = np.zeros(4)
+    p = ctypes.c_void_p(buf.ctypes.data)
+    for count in (1 << 61, (1 << 63) - 1, (8 << 20) // 8 + 1):
+        assert L.dgk_convert_upload_noalloc(p, d.Float64, p, d.Float32, count, None) == _lib.ERR_INVALID
+        assert b"8 MiB" in L.dgk_global_error()
 
 
+@pytest.mark.gpu
 def test_noalloc_upload_matches_runner_upload_twice():
     n = 300_000
     r = Runner(Config(K=[n]))
