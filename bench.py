@@ -43,6 +43,16 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+def peaks_bf16():
+    """Dense bf16 tensor rate in TFLOP/s: the driver-measured burst figure, else the pool's fallback."""
+    try:
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
 def b_alg_mixed(N: int) -> float:
     """Algorithmic bytes per DOF-stage of the mixed stage: hi, lo and resu read and written (FP32), plus the
     compact per-element geometry (8 floats) and connectivity (5 int32) spread over the Np nodes."""
@@ -308,16 +318,27 @@ def run_ensemble(args, world, rank, local):
     E.free()
 
 
+def oz_ops_per_element(N: int, S: int = 6) -> float:
+    """Integer multiply-adds x 2 per element and stage of the exact-digit precision kernel as issued (digit
+    products p + q <= S - 1 over 128 matrix rows and the padded K of the volume, 3 rup32(Np), and LIFT,
+    rup32(4 Nfp))."""
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    Nfp = (N + 1) * (N + 2) // 2
+    r32 = lambda x: (x + 31) // 32 * 32
+    return 2.0 * 128 * (3 * r32(Np) + r32(4 * Nfp)) * S * (S + 1) / 2
+
+
 def run_precision(args, world, rank, local):
-    """Precision workload: order 7, 32^3 x 6 Kuhn mesh, u0 = 0.5 + 0.25 sin(pi x) cos(pi y) sin(pi z), to t = 0.2: the
-    precision form (tcgen05 BF16 hi/lo GEMMs, FP32 accumulation, compensated FP32 state) against the FP64 run.
-    The same run at order 4 is reported beside it: on the reference's order-7 node set the split products lose
-    every digit of the derivative and the run leaves the stable range."""
+    """Precision workload: order 7, 32^3 x 6 Kuhn mesh, u0 = 0.5 + 0.25 sin(pi x) cos(pi y) sin(pi z), to t = 0.2:
+    the precision form (both element-local products as exact 8-bit-digit GEMMs on the tensor cores, six digits
+    per operand joined in FP64, compensated FP32 state) against the plain FP64 run of the same mesh, with L2 and
+    Linf errors at t_final; the same at order 4 beside it."""
     import torch
     from dgkernel_b200.burgers import BurgersProblem, MIXED
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
     n = 32 if args.n == 64 else args.n
+    ops_peak = 2.0 * peaks_bf16()[0]  # dense int8 rate = twice the bf16 rate on B200
     per_order = {}
     for order in (7, 4):
         res = {}
@@ -334,27 +355,35 @@ def run_precision(args, world, rank, local):
                 e1.record(stream)
                 torch.cuda.synchronize()
             res[name] = {"ms": e0.elapsed_time(e1) / (nst - args.warmup), "u": P.get("u"), "dofs": P.dofs,
-                         "stages": nst, "clk": clk.summary()}
+                         "stages": nst, "clk": clk.summary(), "K": P.K}
             P.free()
         ref, tc = res["f64"]["u"], res["tc"]["u"]
         fin = bool(np.isfinite(tc).all())
+        ops = oz_ops_per_element(order) * res["tc"]["K"] / (res["tc"]["ms"] * 1e-3) / 1e12
         per_order[order] = {
             "tc_value": world * res["tc"]["dofs"] / (res["tc"]["ms"] * 1e-3), "tc_ms_per_step": res["tc"]["ms"],
             "fp64_value": world * res["f64"]["dofs"] / (res["f64"]["ms"] * 1e-3), "fp64_ms_per_step": res["f64"]["ms"],
+            "speedup_vs_fp64": res["f64"]["ms"] / res["tc"]["ms"],
             "stages": res["tc"]["stages"], "finite": fin,
             "l2_err_vs_fp64": float(np.linalg.norm(tc - ref) / np.linalg.norm(ref)) if fin else None,
             "linf_err_vs_fp64": float(np.max(np.abs(tc - ref)) / np.max(np.abs(ref))) if fin else None,
+            "int8_tops": ops, "tensor_frac": ops / ops_peak,
             "clocks": res["tc"]["clk"]}
     if rank == 0:
         m = per_order[7]
         out = {"metric": "DOF-stage-updates/s, precision form (order 7, 32^3x6)", "value": m["tc_value"], "unit": UNIT,
                "n_gpus": world, "steps": m["stages"], "warmup": args.warmup, "ms_per_step": m["tc_ms_per_step"],
-               "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3 (fp32 acc)",
+               "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+               "dtype": "i8 digits x6 (exact int32 acc, f64 join), f32x2 state",
                "data": "synthetic",
                "config": {"workload": f"3-D Burgers, order 7 (Np=120), periodic {n}^3x6 Kuhn mesh, u0 = 0.5 + 0.25 "
                                       f"sin cos sin, to t = 0.2; order 4 on the same mesh beside it",
                           "orders": {str(k): {kk: vv for kk, vv in v.items() if kk != "clocks"}
                                      for k, v in per_order.items()}},
+               "roofline": {"bound": "tensor", "achieved": m["int8_tops"], "peak": ops_peak, "unit": "TOPS (int8)",
+                            "frac": m["tensor_frac"], "traffic": None, "kernel": "rhs_stage_oz_kernel",
+                            "peak_kind": "twice the measured bf16 dense rate",
+                            "ops_per_element": oz_ops_per_element(7)},
                "clocks": m["clocks"], "gpu_launches": m["stages"]}
         print(json.dumps(out), flush=True)
 

@@ -19,8 +19,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 CXXFLAGS = ["-O3", "-std=c++17"]
 
-CU = ["kernels.cu", "kernels_tma.cu", "setup.cu", "ops.cu", "noalloc.cu", "mixed.cu", "av.cu", "tc.cu", "tcm.cu"]
-CPP = ["runner.cpp", "element.cpp", "mesh.cpp", "abi.cpp"]
+CU = ["kernels.cu", "kernels_tma.cu", "setup.cu", "ops.cu", "noalloc.cu", "mixed.cu", "av.cu", "tcm.cu", "oz.cu"]
+CPP = ["runner.cpp", "element.cpp", "mesh.cpp", "gambit.cpp", "abi.cpp"]
 
 
 def _run(cmd):

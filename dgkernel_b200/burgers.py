@@ -161,7 +161,7 @@ class _TetBurgers:
         carr = (C.c_char_p * 20)(*[None if v is None else v.encode() for v in names])
         hmin = C.c_double()
         check(lib().dgk_setup_geometry(r._h, el._h, len(VX), _pd(VX), _pd(VY), _pd(VZ), _pi(EToV), _pi(EToE),
-                                       _pi(EToF), 2.0, carr, C.byref(hmin)), r._h)
+                                       _pi(EToF), getattr(self, "period", 2.0), carr, C.byref(hmin)), r._h)
         self.hmin = hmin.value
         # FaceConnector pick/place fused into one gather map over the state array's partition offsets
         self.vmapP = np.zeros(K * NF, dtype=np.int64)
@@ -339,6 +339,43 @@ class BurgersProblem(_TetBurgers):
             modes = random_modes(seed, sigma=mode_sigma) if kind == 2 else np.zeros((0, 5))
             check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, len(modes), _pd(modes)), r._h)
         self._finish(cfl, conservative, warps, ring, eps0, c0, kappa, conf)
+
+
+def partition_order(EToP):
+    """Element order that makes every partition a contiguous block (ascending partition id, then ascending
+    element id: the FaceConnector's local numbering, utils/face_connector.go:93-118), the partition ids in
+    that order, and the element count of each."""
+    EToP = np.asarray(EToP, dtype=np.int64)
+    if EToP.size and EToP.min() < 0:
+        raise ValueError("every element needs a partition (EToP has unassigned elements)")
+    order = np.argsort(EToP, kind="stable")
+    ids, counts = np.unique(EToP, return_counts=True)
+    return order, ids, [int(c) for c in counts]
+
+
+class BurgersMesh(_TetBurgers):
+    """Burgers problem of order N on an unstructured tetrahedral mesh (vertices VX, VY, VZ, EToV [K, 4], optional
+    EToP, e.g. from mesh.read_gambit), not periodic: faces without a neighbour keep VmapP = VmapM
+    (element/library/gonudg/buildmaps3d.go:34, 156-173), so their Lax-Friedrichs difference vanishes.  Elements
+    are stored partition by partition (partition_order); `order` maps stored position -> input element."""
+
+    def __init__(self, N: int, VX, VY, VZ, EToV, EToP=None, dtype=np.float64, u0: str = "sine", cfl: float = 0.3,
+                 conservative: int = 0, stream=None, mma=None, tensor=None):
+        EToV = np.ascontiguousarray(EToV, dtype=np.int64)
+        K = EToV.shape[0]
+        EToP = np.zeros(K, dtype=np.int64) if EToP is None else np.asarray(EToP, dtype=np.int64)
+        order, self.part_ids, Kpart = partition_order(EToP)
+        EToV = np.ascontiguousarray(EToV[order])
+        EToPc = np.ascontiguousarray(np.repeat(np.arange(len(Kpart), dtype=np.int64), Kpart))
+        EToE, EToF = M.ti_connect3d(EToV)
+        self.order, self.period, self.mma, self.tensor = order, 0.0, mma, tensor
+        VX, VY, VZ = (np.ascontiguousarray(v, dtype=np.float64) for v in (VX, VY, VZ))
+        self._assemble(N, VX, VY, VZ, EToV, EToE, EToF, EToPc, Kpart, dtype, stream)
+        kinds = {"sine": (0, 0.0, 0.5), "shock": (0, 0.5, 1.0), "smooth": (1, 0.5, 0.25)}
+        kind, mean, amp = kinds[u0]
+        r = self.runner
+        check(lib().dgk_init_field(r._h, b"u", b"X", b"Y", b"Z", kind, mean, amp, 0, _pd(np.zeros(5))), r._h)
+        self._finish(cfl, conservative)
 
 
 class BurgersEnsemble(_TetBurgers):

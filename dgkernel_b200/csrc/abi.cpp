@@ -216,6 +216,33 @@ int dgk_kuhn_mesh(int32_t n, int32_t nslab, double lo, double hi, double *VX, do
 int dgk_ti_connect3d(int64_t K, const int64_t *EToV, int64_t *EToE, int64_t *EToF) {
   return guard(nullptr, [&] { dgk::ti_connect3d(K, EToV, EToE, EToF); });
 }
+int dgk_read_gambit(const char *path, int64_t *counts, double *VX, double *VY, double *VZ, int64_t *EToV,
+                    int64_t *EToP, int64_t *bfaces) {
+  return guard(nullptr, [&] {
+    if (!path || !counts) throw dgk::Error(DGK_ERR_INVALID, "read gambit: null path or counts");
+    const dgk::GambitMesh m = dgk::read_gambit(path);
+    const int64_t nv = (int64_t)m.VX.size(), ne = (int64_t)m.EToV.size() / 4;
+    counts[0] = nv;
+    counts[1] = ne;
+    counts[2] = (int64_t)m.bfaces.size();
+    counts[3] = m.EToP.empty() ? 0 : 1;
+    if (VX && VY && VZ)
+      for (int64_t i = 0; i < nv; ++i) {
+        VX[i] = m.VX[(size_t)i];
+        VY[i] = m.VY[(size_t)i];
+        VZ[i] = m.VZ[(size_t)i];
+      }
+    if (EToV) std::copy(m.EToV.begin(), m.EToV.end(), EToV);
+    if (EToP && !m.EToP.empty()) std::copy(m.EToP.begin(), m.EToP.end(), EToP);
+    if (bfaces)
+      for (size_t i = 0; i < m.bfaces.size(); ++i) {
+        bfaces[3 * i] = m.bfaces[i].elem;
+        bfaces[3 * i + 1] = m.bfaces[i].face;
+        bfaces[3 * i + 2] = m.bfaces[i].set;
+      }
+  });
+}
+
 int dgk_face_connector(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP, const int64_t *EToP,
                        int32_t npart, int64_t *pick_len, int64_t *pick_idx, int64_t *place_idx) {
   return guard(nullptr, [&] {

@@ -146,25 +146,23 @@ struct SplitJoinArgs {
   float *hi, *lo;
 };
 
-// ---- precision form on the tensor cores (tc.cu) ----
-struct TcArgs {
-  const MTile *tiles;  // tiles of up to 64 elements; elem_slot indexes the compact geometry / connectivity
+// ---- precision form with exact integer products on the tensor cores (oz.cu) ----
+struct OzArgs {
+  const MTile *tiles;  // tiles of up to 32 elements (one compact-geometry slot each)
   int ntiles;
   const float *uhi_in, *ulo_in;
   float *uhi_out, *ulo_out, *resu;
-  const float *geo;          // kMixedGeoWords per element slot
-  const int32_t *conn;       // kMixedConnWords per element slot
-  int64_t n_u_values;
-  const unsigned char *amat; // Dr, Ds, Dt, LIFT as BF16 hi/lo in the canonical K-major layout
-  int64_t aoff[4];           // byte offsets of the four matrices in amat
-  const double *bary;        // [NP][3]
-  const int32_t *vtx;        // vertex nodes A..D
-  const uint8_t *ftab;
-  const int32_t *fmask;
+  const float *geo;             // kMixedGeoWords per element slot
+  const int32_t *conn;          // kMixedConnWords per element slot
+  int64_t n_u_values;           // bound of every gathered value index
+  const unsigned char *amat;    // matrix digits in 4 KB chunks, digit-major (oz_pack_operands)
+  const int32_t *rexp;          // [2][128]: row exponents of the volume and LIFT rows
+  const double *bary;           // [NP][3]
+  const int32_t *vtx;           // vertex nodes A..D
+  const uint8_t *ftab;          // [ncodes][Nfp]
+  const int32_t *fmask;         // [4 Nfp]
   int ncodes;
-  float a, dt;
-  double b;
-  int conservative;
+  double a, b, dt;
   int *status;
 };
 

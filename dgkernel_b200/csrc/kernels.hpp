@@ -48,11 +48,16 @@ template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);
 void launch_split_join(const SplitJoinArgs &a, cudaStream_t st);
 
-// Precision form on the tensor cores (tc.cu): orders 4..7.
-bool launch_rhs_tc(int N, const TcArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info);
-int tc_tile_elems();
-void tc_pack_operands(const double *const *mats, const int *cols, int rows, std::vector<uint16_t> &out,
-                      int64_t off[4]);
+// Precision form with exact integer products on the tensor cores (oz.cu): orders 4..7, tiles of
+// oz_tile_elems() elements; oz_pack_operands lays out the matrix digits and the row exponents (Dr, Ds, Dt,
+// LIFT row-major FP64).
+bool oz_supported(int N);
+int oz_tile_elems();
+int oz_digits();
+void oz_pack_operands(int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
+                      std::vector<uint8_t> &digits, std::vector<int32_t> &rexp);
+void prepare_rhs_oz(int N);  // attributes, before any stream capture
+bool launch_rhs_oz(int N, const OzArgs &A, int conservative, int num_sms, cudaStream_t st, LaunchInfo *info);
 
 // Artificial-viscosity stage and the sensor MLP (av.cu).
 void launch_av(int N, const AvArgs &A, int num_sms, cudaStream_t st);

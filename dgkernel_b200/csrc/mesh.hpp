@@ -1,6 +1,7 @@
 // Host-side mesh setup, see mesh.cpp.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <vector>
 
 namespace dgk {
@@ -32,6 +33,26 @@ struct CompactFaces {
 CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,
                            const int64_t *slot_prefix, int Np, int Nfp, const int32_t *gmap);
 int64_t slot_padded(int64_t k);  // k rounded up to whole 32-element slots
+
+// Gambit neutral file (tetrahedra): vertices in file order, EToV as 0-based vertex positions, EToP from the
+// "p<N>" element groups (empty when the file has at most one group), boundary faces (element, 0-based face,
+// boundary-set index).
+struct GambitGroup {
+  int64_t tag = 0;
+  std::string name;
+  std::vector<int64_t> elements;
+};
+struct GambitFace {
+  int64_t elem, face, set;
+};
+struct GambitMesh {
+  std::vector<double> VX, VY, VZ;
+  std::vector<int64_t> EToV, EToP;
+  std::vector<GambitGroup> groups;
+  std::vector<std::string> bc_names;
+  std::vector<GambitFace> bfaces;
+};
+GambitMesh read_gambit(const std::string &path);
 
 uint64_t splitmix_next(uint64_t &state);
 double splitmix_uniform(uint64_t &state);

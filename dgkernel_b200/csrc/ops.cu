@@ -384,8 +384,7 @@ struct MatmulOp : Op {
 struct MixedOp : Op {
   int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0, tensor = 0, mma = 0;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
-  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat, bmat;
-  int64_t aoff[4] = {0, 0, 0, 0};
+  DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat, rexp, bmat;
   LaunchInfo info;
 
   template <typename G>
@@ -444,10 +443,11 @@ struct MixedOp : Op {
             *fm = R.matrix("Fmask"), *B = R.matrix("Bary");
     const int64_t np = Dr->rows;
     N = order_from_np(np);
-    // orders 6 and 7 (and any order with tensor=1) run the precision form on the tensor cores
+    // orders 6 and 7 (and any order with tensor=1) run the precision form: exact integer-digit products on the
+    // tensor cores
     tensor = R.flag("tensor", N >= 6 ? 1 : 0);
-    if (tensor && (N < 4 || N > 7))
-      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the tensor-core form is built for orders 4..7");
+    if (tensor && !oz_supported(N))
+      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the tensor-core precision form is built for orders 4..7");
     if (!tensor && mixed_slot_bytes(N) == 0)
       throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": the mixed stage is built for orders 1..5");
     // mma=1: the element-local products on the tensor cores with three-part BF16 operands (orders 1..4)
@@ -530,19 +530,19 @@ struct MixedOp : Op {
     std::vector<int32_t> fmi(fm->mat.begin(), fm->mat.end());
     for (int32_t v : fmi) require(v >= 0 && v < np, R.kname + ": Fmask entry out of range");
     fmask.upload(fmi.data(), fmi.size() * sizeof(int32_t));
-    if (tensor) {  // BF16 hi/lo operands of Dr, Ds, Dt and LIFT in the tensor cores' canonical layout
-      const double *mats[4] = {Dr->mat.data(), Ds->mat.data(), Dt->mat.data(), L->mat.data()};
-      const int cols[4] = {(int)np, (int)np, (int)np, nf};
-      std::vector<uint16_t> packed;
-      tc_pack_operands(mats, cols, (int)np, packed, aoff);
-      amat.upload(packed.data(), packed.size() * sizeof(uint16_t));
+    if (tensor) {  // integer digits of Dr, Ds, Dt and LIFT in 4 KB chunks, and their row exponents
+      std::vector<uint8_t> packed;
+      std::vector<int32_t> re;
+      oz_pack_operands(N, Dr->mat.data(), Ds->mat.data(), Dt->mat.data(), L->mat.data(), packed, re);
+      amat.upload(packed.data(), packed.size());
+      rexp.upload(re.data(), re.size() * sizeof(int32_t));
     }
     if (mma) {
       std::vector<uint16_t> packed;
       tcm_pack_operands(N, Dr->mat.data(), Ds->mat.data(), Dt->mat.data(), L->mat.data(), packed);
       bmat.upload(packed.data(), packed.size() * sizeof(uint16_t));
     }
-    const int te = tensor ? tc_tile_elems() : mma ? tcm_tile_elems() : kMixedSlotElems;
+    const int te = tensor ? oz_tile_elems() : mma ? tcm_tile_elems() : kMixedSlotElems;
     std::vector<MTile> tl;
     for (int p = 0; p < P; ++p)
       for (int64_t s0 = 0; s0 < r.K[p]; s0 += te) {
@@ -551,7 +551,7 @@ struct MixedOp : Op {
         x.elem_slot = slot_prefix[p] + s0;
         x.nelem = (int32_t)std::min<int64_t>(te, r.K[p] - s0);
         x.part = p;
-        require(tensor || (x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
+        require((x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
         tl.push_back(x);
       }
     ntiles = (int)tl.size();
@@ -561,11 +561,13 @@ struct MixedOp : Op {
   void prepare(Runner &) override {
     if (mma)
       prepare_rhs_tcm(N, warps);
-    else if (!tensor)
+    else if (tensor)
+      prepare_rhs_oz(N);
+    else
       prepare_rhs_mixed(N, warps);
   }
   void launch_tensor(Runner &r, const std::vector<double> &s) {
-    TcArgs A{};
+    OzArgs A{};
     A.tiles = tiles.get<MTile>();
     A.ntiles = ntiles;
     A.uhi_in = reinterpret_cast<const float *>(uhi->dptr);
@@ -577,19 +579,18 @@ struct MixedOp : Op {
     A.conn = conn.get<int32_t>();
     A.n_u_values = uhi->offsets.back();
     A.amat = amat.get<unsigned char>();
-    for (int c = 0; c < 4; ++c) A.aoff[c] = aoff[c];
+    A.rexp = rexp.get<int32_t>();
     A.bary = bary.get<double>();
     A.vtx = vtx.get<int32_t>();
     A.ftab = ftab.get<uint8_t>();
     A.fmask = fmask.get<int32_t>();
     A.ncodes = ncodes;
-    A.a = (float)s[0];
+    A.a = s[0];
     A.b = s[1];
-    A.dt = (float)s[2];
-    A.conservative = conservative;
+    A.dt = s[2];
     A.status = r.status_word();
-    if (!launch_rhs_tc(N, A, r.num_sms, r.stream(), &info))
-      throw Error(DGK_ERR_UNSUPPORTED, "tensor-core stage: no form for this order");
+    if (!launch_rhs_oz(N, A, conservative, r.num_sms, r.stream(), &info))
+      throw Error(DGK_ERR_UNSUPPORTED, "tensor-core precision stage: shared memory does not fit this order");
     std::swap(uhi->dptr, uhin->dptr);
     std::swap(ulo->dptr, ulon->dptr);
   }

@@ -30,6 +30,25 @@ def kuhn_mesh(n: int, nslab: int = 1, lo: float = -1.0, hi: float = 1.0):
     return VX, VY, VZ, EToV, EToVp, EToP
 
 
+def read_gambit(path: str):
+    """Gambit neutral file (tetrahedra) as read by ReadGambitNeutral (mesh/readers/gambit_reader.go:13-338):
+    dict with VX, VY, VZ (vertices in file order), EToV [K, 4] (0-based), EToP [K] (partition N of the elements
+    of group "p<N>", -1 unassigned) or None when the file has at most one element group, and bfaces [nb, 3]
+    (element, 0-based Gambit face, boundary-set index)."""
+    L = lib()
+    counts = np.zeros(4, dtype=np.int64)
+    p = str(path).encode()
+    check(L.dgk_read_gambit(p, _p(counts, _PI64), None, None, None, None, None, None))
+    nv, K, nb, parts = (int(v) for v in counts)
+    VX, VY, VZ = np.zeros(nv), np.zeros(nv), np.zeros(nv)
+    EToV = np.zeros((K, 4), dtype=np.int64)
+    EToP = np.full(K, -1, dtype=np.int64)
+    bf = np.zeros((nb, 3), dtype=np.int64)
+    check(L.dgk_read_gambit(p, _p(counts, _PI64), _p(VX, _PD), _p(VY, _PD), _p(VZ, _PD), _p(EToV, _PI64),
+                            _p(EToP, _PI64), _p(bf, _PI64) if nb else None))
+    return {"VX": VX, "VY": VY, "VZ": VZ, "EToV": EToV, "EToP": EToP if parts else None, "bfaces": bf}
+
+
 def ti_connect3d(EToV):
     """Element-to-element / element-to-face connectivity (gonudg ticonnect3d.go:24-102)."""
     EToV = np.ascontiguousarray(EToV, dtype=np.int64)

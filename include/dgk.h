@@ -164,6 +164,14 @@ int dgk_element_fmask(const dgk_element *e, int32_t *out);
  * (vertex ids wrapped mod n for periodic face matching) and EToP: 6n^3 entries (EToV 4 per element). */
 int dgk_kuhn_mesh(int32_t n, int32_t nslab, double lo, double hi, double *VX, double *VY, double *VZ,
                   int64_t *EToV, int64_t *EToV_periodic, int64_t *EToP);
+/* Gambit neutral mesh file, tetrahedra only (replaces ReadGambitNeutral, mesh/readers/gambit_reader.go:13-338).
+ * First call with NULL arrays: counts[4] = {vertices, elements, boundary faces, has_partitions}.  Second call
+ * with arrays of those sizes: VX/VY/VZ (vertices in file order), EToV (4 per element, 0-based vertex
+ * positions), EToP (partition N of every element in a group named "p<N>", -1 for unassigned elements; written
+ * only when has_partitions, i.e. the file has more than one element group), bfaces (3 per boundary face:
+ * element, 0-based Gambit face, boundary-set index).  Elements other than 4-node tetrahedra are an error. */
+int dgk_read_gambit(const char *path, int64_t *counts, double *VX, double *VY, double *VZ, int64_t *EToV,
+                    int64_t *EToP, int64_t *bfaces);
 /* tiConnect3D (element/library/gonudg/ticonnect3d.go:24-102). */
 int dgk_ti_connect3d(int64_t K, const int64_t *EToV, int64_t *EToE, int64_t *EToF);
 /* FaceConnector (utils/face_connector.go:43-187).  First call with pick_idx == NULL to get the

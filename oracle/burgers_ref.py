@@ -170,3 +170,40 @@ class Problem:
             raise ValueError(u0)
         self.hmin = h_min(self.X, self.Y, self.Z)
         self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))
+
+
+class MeshProblem(Problem):
+    """The arrays of a Burgers problem on an unstructured tetrahedral mesh (not periodic: unmatched faces keep
+    VmapP = VmapM, buildmaps3d.go:34), elements stored partition by partition in ascending partition id, then
+    ascending element id (the FaceConnector's local numbering), partitions renumbered 0.. in that order."""
+
+    def __init__(self, N: int, VX, VY, VZ, EToV, EToP=None, u0: str = "sine", cfl: float = 0.3):
+        EToV = np.asarray(EToV, dtype=np.int64)
+        K = EToV.shape[0]
+        EToP = np.zeros(K, dtype=np.int64) if EToP is None else np.asarray(EToP, dtype=np.int64)
+        order = np.argsort(EToP, kind="stable")
+        ids, counts = np.unique(EToP, return_counts=True)
+        self.N, self.n, self.nparts = N, 0, len(ids)
+        self.el = g.ref_element(N)
+        self.VX, self.VY, self.VZ = (np.asarray(v, dtype=np.float64) for v in (VX, VY, VZ))
+        self.EToV = EToV[order]
+        self.EToP = np.repeat(np.arange(len(ids), dtype=np.int64), counts)
+        self.order = order
+        self.K = K
+        self.X, self.Y, self.Z = g.node_coords(self.el, self.VX, self.VY, self.VZ, self.EToV)
+        self.geo = g.geometric_factors(self.el, self.X, self.Y, self.Z)
+        self.EToE, self.EToF = g.ti_connect3d(self.EToV)
+        self.vmapM, self.vmapP, self.mapP, self.mapB = g.build_maps3d(self.el, self.X, self.Y, self.Z, self.EToE,
+                                                                      self.EToF, period=None)
+        self.fc = g.face_connector(self.K, 4, self.el.Nfp, self.el.Np, self.vmapP, self.EToP)
+        self.Kpart = [int(v) for v in self.fc.elems_per_part]
+        if u0 == "sine":
+            self.u0 = u0_sine(self.X, self.Y, self.Z)
+        elif u0 == "shock":
+            self.u0 = u0_sine(self.X, self.Y, self.Z, amp=1.0, offset=0.5)
+        elif u0 == "smooth":
+            self.u0 = u0_smooth_c3(self.X, self.Y, self.Z)
+        else:
+            raise ValueError(u0)
+        self.hmin = h_min(self.X, self.Y, self.Z)
+        self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))

@@ -7,6 +7,8 @@ Go test files as text:
   * element/library/gonudg/jacobi_quadrature_test.go  TestJacobiGL table (alpha, beta, N, expected nodes)
   * element/library/gonudg/jacobip_test.go            P_0^(a,0) values and the P_{0,0,0} product
   * utils/mesh_test_helpers.go                        createCubeNodes / createCubeMesh / createTwoTetMesh
+  * mesh/cube-partitioned.neu                         the 565-tet partitioned cube (-> cube_partitioned.json:
+                                                      nodes, elements, groups and boundary sets as lists)
 """
 from __future__ import annotations
 
@@ -18,6 +20,7 @@ import sys
 
 ROOT = ""
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_golden.json")
+MESH_OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cube_partitioned.json")
 
 
 def _go_expr(expr: str) -> float:
@@ -65,6 +68,51 @@ def meshes(text: str):
             "two_tet_nodes": two_nodes, "two_tet_tets": two}
 
 
+def gambit_fixture(text: str):
+    """The partitioned cube mesh as plain lists: nodes [id, x, y, z] and elements [id, n1..n4] in file order,
+    element groups [tag, name, element ids], boundary sets [name, [[element id, face], ...]] (1-based ids)."""
+    lines = text.split("\n")
+    i = next(k for k, l in enumerate(lines) if "NUMNP" in l) + 1
+    numnp, nelem, ngrps, nbsets = (int(x) for x in lines[i].split()[:4])
+    nodes, elements, groups, bcs = [], [], [], []
+    while i < len(lines):
+        t = lines[i].strip()
+        i += 1
+        if "NODAL COORDINATES" in t:
+            for _ in range(numnp):
+                f = lines[i].split()
+                i += 1
+                nodes.append([int(f[0]), float(f[1]), float(f[2]), float(f[3])])
+        elif "ELEMENTS/CELLS" in t:
+            for _ in range(nelem):
+                f = lines[i].split()
+                i += 1
+                elements.append([int(f[0])] + [int(x) for x in f[3:7]])
+        elif "ELEMENT GROUP" in t:
+            f = lines[i].split()
+            tag, count = int(f[f.index("GROUP:") + 1]), int(f[f.index("ELEMENTS:") + 1])
+            name = lines[i + 1].strip()
+            i += 3
+            els = []
+            while len(els) < count:
+                els += [int(x) for x in lines[i].split()]
+                i += 1
+            groups.append([tag, name, els])
+        elif "BOUNDARY CONDITIONS" in t:
+            for _ in range(nbsets):
+                f = lines[i].split()
+                i += 1
+                ents = []
+                for _ in range(int(f[2])):
+                    e = lines[i].split()
+                    i += 1
+                    ents.append([int(e[0]), int(e[2])])
+                bcs.append([f[0], ents])
+    assert len(groups) == ngrps
+    return {"source": "mesh/cube-partitioned.neu of DGKernel, extracted by tests/golden/make_golden.py",
+            "nodes": nodes, "elements": elements, "groups": groups, "bcs": bcs}
+
+
 def main():
     global ROOT
     ROOT = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("DGK_REFERENCE_ROOT", "")
@@ -87,6 +135,11 @@ def main():
     }
     with open(OUT, "w") as f:
         json.dump(out, f, indent=1)
+    with open(os.path.join(ROOT, "mesh", "cube-partitioned.neu")) as f:
+        fx = gambit_fixture(f.read())
+    with open(MESH_OUT, "w") as f:
+        json.dump(fx, f, separators=(",", ":"))
+    print(f"wrote {MESH_OUT}: {len(fx['nodes'])} nodes, {len(fx['elements'])} tets, {len(fx['groups'])} groups")
     print(f"wrote {OUT}: {len(out['jacobi_gl'])} JacobiGL cases, {len(out['jacobi_p'])} JacobiP values")
 
 

@@ -2,7 +2,7 @@
 oracle/precision_ref.py; no GPU).
 
 The mixed stage on the tensor cores splits every operand into three BF16 parts and keeps the six products
-a_p b_q with p + q <= 2; the precision form splits into two parts and keeps three products.  Stated bounds, on
+a_p b_q with p + q <= 2; a two-part split (three products) is kept for comparison.  Stated bounds, on
 order-4 reference matrices and random operands of both signs:
   * a three-part split reconstructs an FP32 value to 2^-24 of its magnitude (each part is the BF16 rounding of
     an exact FP32 remainder; the last remainder is at most half a BF16 ulp of the second);
@@ -66,3 +66,20 @@ def test_three_part_rhs_matches_fp64_rhs():
     got = PR.rhs(ref, hi, lo, parts=3).astype(np.float64).reshape(-1)
     err = np.linalg.norm(got - exact) / np.linalg.norm(exact)
     assert err < 1e-6, err
+
+
+def test_exact_digit_products_reach_47_bits():
+    """The integer-digit products of the precision form (six digits per operand, exact digit sums): the digits
+    keep every operand row to 2^-47 of its largest entry (floor digits: the remainder is non-negative) and
+    the dropped digit products p + q >= 6 stay below 7 * 2^-46, so against the FP64 product of order-7
+    reference matrices and operands of both signs and varied scales the error is below
+    2^-42 K max|a_row| max|b_row| (measured 2^-43.6)."""
+    ref = b.Problem(7, 2, 1, "smooth")
+    el = ref.el
+    rng = np.random.default_rng(3)
+    X = rng.standard_normal((40, el.Np)) * np.exp(rng.uniform(-8, 2, (40, 1)))
+    for M in (el.Dr, el.LIFT[:, :el.Np]):
+        want = X @ M.T
+        got = PR.exact_prod(M, X, 6)
+        scale = M.shape[1] * np.abs(X).max(axis=1)[:, None] * np.abs(M).max(axis=1)[None, :]
+        assert np.max(np.abs(got - want) / scale) < 2.0 ** -42
