@@ -10,13 +10,15 @@
 // applications", Numerical Algorithms 59, 2012; on integer units: Uchino, Ozaki and Imamura, "Performance
 // enhancement of the Ozaki scheme on integer matrix multiplication unit", IJHPCA 2025):
 //
-//   every row x of an operand is scaled by a power of two 2^E with |x| < 2^E and cut into S digits,
-//   x = 2^(E-7) (d_0 + 2^-8 (d_1 + 2^-8 (d_2 + ...))), d_0 = floor(x 2^(7-E)) in [-128, 127] (s8) and
-//   d_p in [0, 255] (u8) for p > 0; the digit products d^A_p d^B_q with p + q = L summed over K are exact in
+//   every row x of an operand is scaled by a power of two 2^E with |x| < 2^E, rounded once to the integer
+//   n = rint(x 2^(B-E)) with B = 7 + 8 (S - 1) bits and cut into S digits, x ~ 2^(E-7) (d_0 + 2^-8 (d_1 + ...)),
+//   d_0 = n >> (B - 7) in [-128, 127] (s8) and the bytes d_p in [0, 255] (u8) for p > 0 (exact integer shifts;
+//   a floating-point remainder loop is not exact: for a tiny negative x, x - floor(x) rounds to 1); the digit
+//   products d^A_p d^B_q with p + q = L summed over K are exact in
 //   int32 (|sum| < 6 * 544 * 255^2 < 2^31), one TMEM accumulator per level L < S; the levels are joined in
 //   FP64 by Horner's rule, h = acc_{S-1}; h = h 2^-8 + acc_L, and scaled by 2^(E_A + E_B - 14).
-//   The terms with p + q >= S are dropped: the product's error is below about S 2^(-8S+1) of
-//   2^(E_A+E_B) sum_K 1, i.e. ~47 bits for S = 6.
+//   The operands carry B = 47 bits (S = 6) rounded to nearest, and the dropped terms p + q >= S stay below
+//   about S 2^(-8S+2) of 2^(E_A+E_B) K.
 //
 // Orientation: the matrices are the MMA's A operand (M = 128 rows = output nodes, rows past Np zero) and the
 // elements its B operand (N = 32 elements per tile), so TMEM lane i holds node i and column e element e, and
@@ -117,9 +119,13 @@ __device__ __forceinline__ void tc_mma_i8(uint32_t tmem, uint64_t da, uint64_t d
       "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
-// Digits of 16 values scaled by 2^-E: digit p of value v at byte v of out[p] (p = 0: s8, p > 0: u8).
+// Digits of 16 values of a row with exponent E: each value rounded once to the integer n = rint(x 2^(B-E)),
+// B = 7 + 8 (S - 1) (|n| <= 2^B; clamped to 2^B - 1 at the top), then cut by arithmetic shifts, which is exact:
+// digit 0 = n >> (B - 7) in [-128, 127] (s8), digit p > 0 = the byte (n >> 8 (S - 1 - p)) & 255 (u8).  `scale`
+// is 2^(B-E).  Digit p of value v goes to byte v of out[p].
 template <int S>
 __device__ __forceinline__ void digits16(const double (&x)[16], double scale, uint4 (&out)[S]) {
+  constexpr int B = 7 + 8 * (S - 1);
   uint32_t w[S][4];
 #pragma unroll
   for (int p = 0; p < S; ++p)
@@ -127,17 +133,11 @@ __device__ __forceinline__ void digits16(const double (&x)[16], double scale, ui
     for (int q = 0; q < 4; ++q) w[p][q] = 0;
 #pragma unroll
   for (int v = 0; v < 16; ++v) {
-    double r = x[v] * scale * 128.0;  // in (-128, 128): exact scaling by powers of two
-    double d = floor(r);
-    w[0][v >> 2] |= ((uint32_t)((int)d) & 0xffu) << (8 * (v & 3));
-    r -= d;  // [0, 1), exact
+    long long n = __double2ll_rn(x[v] * scale);  // |x scale| < 2^B: exact scaling, one rounding
+    n = min(n, (1ll << B) - 1);
 #pragma unroll
-    for (int p = 1; p < S; ++p) {
-      r *= 256.0;
-      d = floor(r);
-      w[p][v >> 2] |= ((uint32_t)d & 0xffu) << (8 * (v & 3));
-      r -= d;
-    }
+    for (int p = 0; p < S; ++p)
+      w[p][v >> 2] |= ((uint32_t)(n >> (8 * (S - 1 - p))) & 0xffu) << (8 * (v & 3));
   }
 #pragma unroll
   for (int p = 0; p < S; ++p) out[p] = make_uint4(w[p][0], w[p][1], w[p][2], w[p][3]);
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
       // issue the next fill if its tile exists and its slot is free (no wait)
       auto try_fill = [&]() {
         if (blockIdx.x + nfill * G >= A.ntiles) return;
-        if (nfill >= 2 && !mbar_try_wait(&sdone[nfill & 1], (uint32_t)((nfill - 2) >> 1) & 1u)) return;
+        if (nfill >= 2 && !mbar_test_wait(&sdone[nfill & 1], (uint32_t)((nfill - 2) >> 1) & 1u)) return;
         issue_fill();
       };
       try_fill();
@@ -267,7 +267,7 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
           if (g >= kOzRing) {
             const uint32_t par = (uint32_t)((g / kOzRing) - 1) & 1u;
             uint32_t it = 0;
-            while (!mbar_try_wait(&aemp[rs], par)) {
+            while (!mbar_test_wait(&aemp[rs], par)) {
               try_fill();
               if (++it >= kSpinLimit) {
                 bad = true;
@@ -416,13 +416,16 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
       const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords);
       const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords + 4);
       const double cd[3] = {(double)g0.x, (double)g0.y, (double)g0.z};
+      // element arithmetic in FP64 without contraction (dmul/dadd): every rounding is the restatement's, so the
+      // digits, which feed an ill-conditioned product at high order, match it exactly
       const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
       const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
-      const double wA = CONS ? 0.5 * uA * uA : uA;
-      const double dB = (CONS ? 0.5 * uB * uB : uB) - wA;
-      const double dC = (CONS ? 0.5 * uC * uC : uC) - wA;
-      const double dD = (CONS ? 0.5 * uD * uD : uD) - wA;
-      if (valid && xg == 0) sL0[eb] = 0.5 * (cd[0] * dB + cd[1] * dC + cd[2] * dD);
+      const double wA = CONS ? __dmul_rn(0.5 * uA, uA) : uA;
+      const double dB = (CONS ? __dmul_rn(0.5 * uB, uB) : uB) - wA;
+      const double dC = (CONS ? __dmul_rn(0.5 * uC, uC) : uC) - wA;
+      const double dD = (CONS ? __dmul_rn(0.5 * uD, uD) : uD) - wA;
+      if (valid && xg == 0)
+        sL0[eb] = 0.5 * __dadd_rn(__dadd_rn(__dmul_rn(cd[0], dB), __dmul_rn(cd[1], dC)), __dmul_rn(cd[2], dD));
       double val[GPT][16];
       double mv = 0.0, ml = 0.0;
       bool badg = false;
@@ -439,8 +442,10 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
             const int j = 16 * x + v;
             if (j < NP) {
               const double uj = (double)hi[j] + (double)lo[j];
-              const double wj = CONS ? 0.5 * uj * uj : uj;
-              const double dw = (wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD);
+              const double wj = CONS ? __dmul_rn(0.5 * uj, uj) : uj;
+              const double lin = __dadd_rn(__dadd_rn(__dmul_rn(sBary[3 * j], dB), __dmul_rn(sBary[3 * j + 1], dC)),
+                                           __dmul_rn(sBary[3 * j + 2], dD));
+              const double dw = (wj - wA) - lin;
               val[gi][v] = dw;
               mv = fmax(mv, fabs(dw));
             }
@@ -468,7 +473,8 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
               }
               const float gf = f == 0 ? g0.w : f == 1 ? g1.x : f == 2 ? g1.y : g1.z;
               const double gg = (double)gf, d = uM - uP;
-              const double fl = 0.5 * d * (0.5 * (uM + uP) * gg - fmax(fabs(uM), fabs(uP)) * fabs(gg));
+              const double fl = __dmul_rn(0.5 * d, __dsub_rn(__dmul_rn(0.5 * (uM + uP), gg),
+                                                            __dmul_rn(fmax(fabs(uM), fabs(uP)), fabs(gg))));
               val[gi][v] = fl;
               ml = fmax(ml, fabs(fl));
             }
@@ -483,7 +489,8 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
       }
       asm volatile("bar.sync 1, %0;" ::"n"(NTH) : "memory");
       if (valid) {
-        const double sv = pow2(-sEv[eb]), sl = pow2(-sEl[eb]);
+        constexpr int BITS = 7 + 8 * (S - 1);
+        const double sv = pow2(BITS - sEv[eb]), sl = pow2(BITS - sEl[eb]);
 #pragma unroll
         for (int gi = 0; gi < GPT; ++gi) {
           const int x = xg + 16 * gi;
@@ -547,13 +554,13 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
           const int e = e0 + q;
           if (e < ne) {
             const int o = e * NP + node;
-            const double dd = hv[q] * pow2(sEv[e] + fv - 14) + sL0[e];
-            const double lf = hl[q] * pow2(sEl[e] + flx - 14);
+            const double dd = __dadd_rn(__dmul_rn(hv[q], pow2(sEv[e] + fv - 14)), sL0[e]);
+            const double lf = __dmul_rn(hl[q], pow2(sEl[e] + flx - 14));
             const double u = (double)sHi[o] + (double)sLo[o];
-            const double rhs = (CONS ? -dd : -u * dd) + lf;
+            const double rhs = __dadd_rn(CONS ? -dd : -__dmul_rn(u, dd), lf);
             const int64_t gi = slot0 + o;
-            const float rn = (float)(a * (double)A.resu[gi] + dt * rhs);
-            const double un = u + b * (double)rn;
+            const float rn = (float)__dadd_rn(__dmul_rn(a, (double)A.resu[gi]), __dmul_rn(dt, rhs));
+            const double un = __dadd_rn(u, __dmul_rn(b, (double)rn));
             const float hn = (float)un;
             A.uhi_out[gi] = hn;
             A.ulo_out[gi] = (float)(un - (double)hn);
@@ -603,21 +610,17 @@ bool launch_oz_n(const OzArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info
   return true;
 }
 
-// Digits of one row scaled by 2^-E, the same arithmetic as the kernel's digits16.
+// Digits of one row with exponent E, the same arithmetic as the kernel's digits16: n = rint(x 2^(B-E)),
+// digit 0 = n >> (B - 7), digit p > 0 = the byte (n >> 8 (S - 1 - p)) & 255.
 void row_digits(const double *x, int n, int E, int S, std::vector<std::vector<int>> &d) {
+  const int B = 7 + 8 * (S - 1);
   d.assign((size_t)S, std::vector<int>((size_t)n, 0));
-  const double scale = std::ldexp(1.0, -E);
+  const double scale = std::ldexp(1.0, B - E);
   for (int v = 0; v < n; ++v) {
-    double r = x[v] * scale * 128.0;
-    double q = std::floor(r);
-    d[0][(size_t)v] = (int)q;
-    r -= q;
-    for (int p = 1; p < S; ++p) {
-      r *= 256.0;
-      q = std::floor(r);
-      d[(size_t)p][(size_t)v] = (int)q;
-      r -= q;
-    }
+    long long q = std::llrint(x[v] * scale);
+    q = std::min(q, (1ll << B) - 1);
+    d[0][(size_t)v] = (int)(q >> (B - 7));
+    for (int p = 1; p < S; ++p) d[(size_t)p][(size_t)v] = (int)((q >> (8 * (S - 1 - p))) & 0xff);
   }
 }
 

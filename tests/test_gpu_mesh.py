@@ -45,7 +45,7 @@ def test_partitioned_cube_fp64_stages_match_oracle(cube, N):
     assert P.Kpart == ref.Kpart == [142, 141, 141, 141] and P.part_ids.tolist() == [1, 2, 3, 4]
     assert np.array_equal(P.order, ref.order)
     assert np.array_equal(P.vmapP, ref.vmapP)
-    assert abs(P.dt - ref.dt) < 1e-15 * ref.dt
+    assert abs(P.dt - ref.dt) < 1e-14 * ref.dt  # h_min from GPU and numpy node coordinates
     u0 = P.u0.copy()
     assert rel_l2(u0, ref.u0) < 1e-15
     P.run_stages(10)

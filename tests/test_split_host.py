@@ -70,10 +70,9 @@ def test_three_part_rhs_matches_fp64_rhs():
 
 def test_exact_digit_products_reach_47_bits():
     """The integer-digit products of the precision form (six digits per operand, exact digit sums): the digits
-    keep every operand row to 2^-47 of its largest entry (floor digits: the remainder is non-negative) and
-    the dropped digit products p + q >= 6 stay below 7 * 2^-46, so against the FP64 product of order-7
-    reference matrices and operands of both signs and varied scales the error is below
-    2^-42 K max|a_row| max|b_row| (measured 2^-43.6)."""
+    keep every operand row to 2^-48 of its largest entry (one rounding to nearest) and the dropped digit
+    products p + q >= 6 stay below 7 * 2^-46, so against the FP64 product of order-7 reference matrices and
+    operands of both signs and varied scales the error is below 2^-42 K max|a_row| max|b_row|."""
     ref = b.Problem(7, 2, 1, "smooth")
     el = ref.el
     rng = np.random.default_rng(3)
@@ -83,3 +82,17 @@ def test_exact_digit_products_reach_47_bits():
         got = PR.exact_prod(M, X, 6)
         scale = M.shape[1] * np.abs(X).max(axis=1)[:, None] * np.abs(M).max(axis=1)[None, :]
         assert np.max(np.abs(got - want) / scale) < 2.0 ** -42
+
+
+def test_digits_in_range_for_tiny_entries():
+    """Digits stay in their 8-bit ranges (s8 first, u8 after) when a row mixes O(1) values with tiny ones of
+    either sign (a floating-point remainder loop would round -1e-18 + 1 to 1 and produce the digit 256), and
+    they reconstruct every value to half a unit of the last digit."""
+    X = np.array([[1.0, -1.4e-18, 2.5e-17, -0.999999999999, 0.5, -3e-300, 0.0]])
+    for S in (4, 6, 7):
+        E, d = PR.digits(X, S)
+        assert d[0].min() >= -128 and d[0].max() <= 127
+        assert all(x.min() >= 0 and x.max() <= 255 for x in d[1:])
+        B = 7 + 8 * (S - 1)
+        rec = sum(d[p].astype(np.float64) * 2.0 ** (-7 - 8 * p) for p in range(S)) * 2.0 ** E[:, None]
+        assert np.max(np.abs(rec - X)) <= 2.0 ** (E.max() - B - 1)
