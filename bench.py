@@ -345,7 +345,7 @@ def run_precision(args, world, rank, local):
         for name, dt in (("f64", np.float64), ("tc", MIXED)):
             P = BurgersProblem(order, n, 1, dt, "smooth", stream=stream.cuda_stream,
                                tensor=True if dt == MIXED else None)
-            nst = 5 * int(np.ceil(0.2 / P.dt))
+            nst = max(5 * int(np.ceil(args.t_final / P.dt)), args.warmup + 5)
             P.run_stages(args.warmup)
             torch.cuda.synchronize()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -377,7 +377,7 @@ def run_precision(args, world, rank, local):
                "dtype": "i8 digits x6 (exact int32 acc, f64 join), f32x2 state",
                "data": "synthetic",
                "config": {"workload": f"3-D Burgers, order 7 (Np=120), periodic {n}^3x6 Kuhn mesh, u0 = 0.5 + 0.25 "
-                                      f"sin cos sin, to t = 0.2; order 4 on the same mesh beside it",
+                                      f"sin cos sin, to t = {args.t_final}; order 4 on the same mesh beside it",
                           "orders": {str(k): {kk: vv for kk, vv in v.items() if kk != "clocks"}
                                      for k, v in per_order.items()}},
                "roofline": {"bound": "tensor", "achieved": m["int8_tops"], "peak": ops_peak, "unit": "TOPS (int8)",
@@ -468,6 +468,7 @@ def main():
     ap.add_argument("--slabs", type=int, default=16)
     ap.add_argument("--e2e-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--t-final", type=float, default=0.2, help="precision workload: final time (0.2)")
     ap.add_argument("--workload", default="burgers", choices=["burgers", "ensemble", "learned", "precision"],
                     help="burgers: order 4, 64^3x6 (default); precision: order 7, 32^3x6; ensemble: 256 order-3 "
                          "instances; learned: order 4, 48^3x6 shock with the learned sensor")

@@ -56,7 +56,8 @@ namespace {
 
 constexpr int kOzTE = 32;         // elements per tile (the MMA's N; one compact-geometry slot)
 constexpr int kOzCW = 16;         // consumer warps
-constexpr int kOzRing = 8;        // matrix-chunk ring slots
+constexpr int kOzRing = 16;       // matrix-chunk ring slots (64 KB in flight: covers the L2 latency)
+constexpr int kOzSlots = 1;       // state slots: released after the digits are built, refilled during the MMAs
 constexpr int kOzChunk = 4096;    // bytes of one matrix chunk: 128 rows x 32 K
 constexpr int kOzTmemCols = 512;
 constexpr int kOzDigits = 6;      // S: digits per operand (~47 significant bits)
@@ -80,12 +81,12 @@ struct OzCfg {
   static constexpr uint32_t OFF_B = 0;
   static constexpr uint32_t OFF_RING = OFF_B + S * BSLICE;
   static constexpr uint32_t OFF_SLOT = OFF_RING + kOzRing * kOzChunk;
-  static constexpr uint32_t OFF_BARY = OFF_SLOT + 2 * SLOT_B;
+  static constexpr uint32_t OFF_BARY = OFF_SLOT + kOzSlots * SLOT_B;
   static constexpr uint32_t OFF_L0 = OFF_BARY + NP * 3 * 8;               // double per element, 2 tile buffers
   static constexpr uint32_t OFF_EXP = OFF_L0 + 2 * kOzTE * 8;             // int: Ev[2][32], El[2][32], Fv[128], Fl[128]
   static constexpr uint32_t OFF_BARS = OFF_EXP + (4 * kOzTE + 2 * 128) * 4;
-  // full[2], sdone[2], aful[R], aemp[R], bful, accf, tfree
-  static constexpr int NBARS = 4 + 2 * kOzRing + 3;
+  // full[NS], sdone[NS], aful[R], aemp[R], bful, accf, tfree
+  static constexpr int NBARS = 2 * kOzSlots + 2 * kOzRing + 3;
   static constexpr uint32_t OFF_MISC = OFF_BARS + NBARS * 8;              // abort flag, TMEM base
   static constexpr uint32_t OFF_PT = (OFF_MISC + 16 + 15) & ~15u;         // per face point: own node, face
   static constexpr uint32_t OFF_FTAB = OFF_PT + ((2 * NF + 15) & ~15);    // face-order rows of 64 bytes
@@ -155,6 +156,15 @@ __device__ __forceinline__ void tmem_ld8i(uint32_t taddr, int (&v)[8]) {
   for (int j = 0; j < 8; ++j) v[j] = (int)r[j];
 }
 
+// 8 consecutive TMEM columns (int32) of this warp's lanes, without waiting: complete with tmem_wait_ld().
+__device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, int (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ int vload(const int *p) { return *reinterpret_cast<const volatile int *>(p); }
 
 // Named barrier `id` over `n` threads that also ORs a predicate across them: every participant gets the same
@@ -184,7 +194,7 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
   // per-tile element exponents and L0, double-buffered by tile parity: tile k writes buffer k & 1 while the
   // epilogue of tile k - 1 may still read the other
   int *sEv2 = reinterpret_cast<int *>(sm + C::OFF_EXP), *sEl2 = sEv2 + 2 * TE, *sFv = sEl2 + 2 * TE, *sFl = sFv + 128;
-  uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *sdone = full + 2, *aful = full + 4,
+  uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *sdone = full + kOzSlots, *aful = sdone + kOzSlots,
            *aemp = aful + kOzRing, *bful = aemp + kOzRing, *accf = bful + 1, *tfree = bful + 2;
   int *sMisc = reinterpret_cast<int *>(sm + C::OFF_MISC);  // [0] abort flag, [1] TMEM base
   uint8_t *sPt = sm + C::OFF_PT;                           // [m] own node of face point m, [NF + m] its face
@@ -204,7 +214,7 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
   for (int x = tid; x < A.ncodes * 64; x += blockDim.x)
     sFt[x] = (x & 63) < NFP ? A.ftab[(x >> 6) * NFP + (x & 63)] : 0;
   if (tid == 0) {
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < kOzSlots; ++b) {
       mbar_init(&full[b], 1);
       mbar_init(&sdone[b], NTH);
     }
@@ -237,7 +247,7 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
       int nfill = 0;  // state fills issued (tiles 0 .. nfill - 1)
       int64_t g = 0;  // matrix chunks issued
       auto issue_fill = [&]() {
-        const int k = nfill, s = k & 1;
+        const int k = nfill, s = k % kOzSlots;
         const MTile tl = A.tiles[blockIdx.x + k * G];
         unsigned char *slot = slots + (size_t)s * C::SLOT_B;
         const uint32_t nb = round16((uint32_t)(tl.nelem * NP * 4));
@@ -254,11 +264,12 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
       // issue the next fill if its tile exists and its slot is free (no wait)
       auto try_fill = [&]() {
         if (blockIdx.x + nfill * G >= A.ntiles) return;
-        if (nfill >= 2 && !mbar_test_wait(&sdone[nfill & 1], (uint32_t)((nfill - 2) >> 1) & 1u)) return;
+        if (nfill >= kOzSlots &&
+            !mbar_test_wait(&sdone[nfill % kOzSlots], (uint32_t)((nfill - kOzSlots) / kOzSlots) & 1u))
+          return;
         issue_fill();
       };
-      try_fill();
-      try_fill();
+      for (int i = 0; i < kOzSlots; ++i) try_fill();
       for (int k = 0; !bad; ++k) {
         const int t = blockIdx.x + k * G;
         if (t >= A.ntiles) break;
@@ -300,9 +311,9 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
         *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
       }
       // drain: the newest fill of each state slot and of each ring slot must land before the CTA leaves
-      for (int s = 0; s < 2 && s < nfill; ++s) {
-        const int kl = s + ((nfill - 1 - s) >> 1) * 2;
-        mbar_wait_bounded(&full[s], (uint32_t)(kl >> 1) & 1u, kSpinLimit);
+      for (int s = 0; s < kOzSlots && s < nfill; ++s) {
+        const int kl = s + ((nfill - 1 - s) / kOzSlots) * kOzSlots;
+        mbar_wait_bounded(&full[s], (uint32_t)(kl / kOzSlots) & 1u, kSpinLimit);
       }
       for (int64_t gl = g > kOzRing ? g - kOzRing : 0; gl < g; ++gl)
         mbar_wait_bounded(&aful[gl % kOzRing], (uint32_t)(gl / kOzRing) & 1u, kSpinLimit);
@@ -387,17 +398,17 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
     for (int k = 0;; ++k) {
       const int t = blockIdx.x + k * G;
       if (t >= A.ntiles) break;
-      const int s = k & 1;
+      const int s = k % kOzSlots, tb = k & 1;  // state slot; tile-parity buffer of exponents and L0
       const MTile tl = tl_next;
       if (t + G < A.ntiles) tl_next = A.tiles[t + G];
       const int ne = tl.nelem;
-      int *sEv = sEv2 + s * TE, *sEl = sEl2 + s * TE;
-      double *sL0 = sL02 + s * TE;
+      int *sEv = sEv2 + tb * TE, *sEl = sEl2 + tb * TE;
+      double *sL0 = sL02 + tb * TE;
       if (tid < TE) {  // buffer s was last read by the epilogue of tile k - 2, finished before the last barrier
         sEv[tid] = -1100;
         sEl[tid] = -1100;
       }
-      const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
+      const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k / kOzSlots) & 1u, kSpinLimit);
       if (bar_or(1, NTH, pend || !got || vload(&sMisc[0]) != 0)) {
         failed = true;
         break;
@@ -450,27 +461,35 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
               mv = fmax(mv, fabs(dw));
             }
           }
-        } else {  // the Lax-Friedrichs flux at face points 16 (x - XV) ..
+        } else {  // the Lax-Friedrichs flux at face points 16 (x - XV) ..: all gathers first, then the math
+          float pH[16], pL[16];
 #pragma unroll
           for (int v = 0; v < 16; ++v) {
             const int m = 16 * (x - XV) + v;
+            pH[v] = 0.f;
+            pL[v] = 0.f;
             if (m < NF) {
               const int f = sPt[NF + m], pp = m - f * NFP;
               const uint32_t nbs = (uint32_t)sCon[ee * kMixedConnWords + f];
               const int cdx = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
               const uint32_t idx = nbs + sFt[cdx * 64 + pp];
-              const uint32_t loc = idx - (uint32_t)slot0;
-              const int own = sPt[m];
-              const double uM = (double)hi[own] + (double)lo[own];
-              double uP;
-              if (loc < (uint32_t)slotn) {
-                uP = (double)sHi[loc] + (double)sLo[loc];
-              } else if (idx < n_u32) {
-                uP = (double)__ldg(A.uhi_in + idx) + (double)__ldg(A.ulo_in + idx);
-              } else {
+              if (idx < n_u32) {
+                pH[v] = __ldg(A.uhi_in + idx);
+                pL[v] = __ldg(A.ulo_in + idx);
+              } else {  // out of range: reported, and the point takes its own trace (zero jump)
                 badg = true;
-                uP = uM;
+                pH[v] = hi[sPt[m]];
+                pL[v] = lo[sPt[m]];
               }
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < 16; ++v) {
+            const int m = 16 * (x - XV) + v;
+            if (m < NF) {
+              const int f = sPt[NF + m], own = sPt[m];
+              const double uM = (double)hi[own] + (double)lo[own];
+              const double uP = (double)pH[v] + (double)pL[v];
               const float gf = f == 0 ? g0.w : f == 1 ? g1.x : f == 2 ? g1.y : g1.z;
               const double gg = (double)gf, d = uM - uP;
               const double fl = __dmul_rn(0.5 * d, __dsub_rn(__dmul_rn(0.5 * (uM + uP), gg),
@@ -523,6 +542,7 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
       fence_async_smem();  // the digits are read by the tensor cores (async proxy)
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(bful);
+      mbar_arrive(&sdone[s]);  // the state slot may be refilled (the epilogue reads the state from global)
 
       // ---- epilogue: join the levels, the stage update ----
       const bool done = mbar_wait_bounded(accf, (uint32_t)k & 1u, kSpinLimit);
@@ -531,18 +551,41 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
         pend = true;  // no TMEM reads; the others learn of it at the next barrier
         continue;
       }
+      // this thread's state and residual first (coalesced over the lanes' nodes), then the accumulators
+      float rs[8], hs[8], ls[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        rs[q] = hs[q] = ls[q] = 0.f;
+        const int e = e0 + q;
+        if (node < NP && e < ne) {
+          const int64_t gi = slot0 + e * NP + node;
+          rs[q] = A.resu[gi];
+          hs[q] = __ldg(A.uhi_in + gi);
+          ls[q] = __ldg(A.ulo_in + gi);
+        }
+      }
+      // Horner over the levels, highest first, loading TMEM in batches of up to three levels per wait
       double hv[8], hl[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) hv[q] = hl[q] = 0.0;
 #pragma unroll
-      for (int L = S - 1; L >= 0; --L) {
-        int av[8], al[8];
-        tmem_ld8i(lane_tmem + (uint32_t)((L * 2) * TE + e0), av);
-        tmem_ld8i(lane_tmem + (uint32_t)((L * 2 + 1) * TE + e0), al);
+      for (int acc = 0; acc < 2; ++acc) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          hv[q] = fma(hv[q], 0.00390625, (double)av[q]);
-          hl[q] = fma(hl[q], 0.00390625, (double)al[q]);
+        for (int L0b = S - 1; L0b >= 0; L0b -= 3) {
+          int av[3][8];
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+            if (L0b - j >= 0) tmem_ld8_nowait(lane_tmem + (uint32_t)(((L0b - j) * 2 + acc) * TE + e0), av[j]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 3; ++j)
+            if (L0b - j >= 0) {
+#pragma unroll
+              for (int q = 0; q < 8; ++q) {
+                double &h = acc ? hl[q] : hv[q];
+                h = fma(h, 0.00390625, (double)av[j][q]);
+              }
+            }
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -553,13 +596,12 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
         for (int q = 0; q < 8; ++q) {
           const int e = e0 + q;
           if (e < ne) {
-            const int o = e * NP + node;
             const double dd = __dadd_rn(__dmul_rn(hv[q], pow2(sEv[e] + fv - 14)), sL0[e]);
             const double lf = __dmul_rn(hl[q], pow2(sEl[e] + flx - 14));
-            const double u = (double)sHi[o] + (double)sLo[o];
+            const double u = (double)hs[q] + (double)ls[q];
             const double rhs = __dadd_rn(CONS ? -dd : -__dmul_rn(u, dd), lf);
-            const int64_t gi = slot0 + o;
-            const float rn = (float)__dadd_rn(__dmul_rn(a, (double)A.resu[gi]), __dmul_rn(dt, rhs));
+            const int64_t gi = slot0 + e * NP + node;
+            const float rn = (float)__dadd_rn(__dmul_rn(a, (double)rs[q]), __dmul_rn(dt, rhs));
             const double un = __dadd_rn(u, __dmul_rn(b, (double)rn));
             const float hn = (float)un;
             A.uhi_out[gi] = hn;
@@ -568,7 +610,6 @@ __global__ void __launch_bounds__(32 * (kOzCW + 2), 1) rhs_stage_oz_kernel(const
           }
         }
       }
-      mbar_arrive(&sdone[s]);  // the state slot may be refilled
     }
     failed = failed || pend;
     if (failed && lane == 0) {

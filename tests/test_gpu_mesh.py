@@ -3,7 +3,8 @@ cube's boundary without a neighbour) through the library's Gambit reader and the
 oracle.  Elements are stored partition by partition; boundary faces keep VmapP = VmapM
 (element/library/gonudg/buildmaps3d.go:34).  Bounds: VmapP bit-exact; FP64 stage <= 1e-12 relative L2 after 10
 LSERK4 stages at orders 1..4; the mixed forms within their stated bounds of the oracle's FP64 run (FP32-FMA
-and three-part BF16 tensor-core products 1e-7, exact-digit precision form 1e-9 at order 4)."""
+and three-part BF16 tensor-core products 1e-7, exact-digit precision form 8e-10 at order 4, twice its measured
+3.9e-10)."""
 import json
 import os
 
@@ -64,5 +65,5 @@ def test_partitioned_cube_mixed_forms(cube, form):
     P.run_stages(10)
     err = rel_l2(P.get("u"), _oracle(ref, u0, P.dt, 10))
     print(f"{form}: relative L2 vs oracle {err:.3e}")
-    assert err < (1e-9 if form == "precision" else 1e-7), err
+    assert err < (8e-10 if form == "precision" else 1e-7), err
     P.free()
