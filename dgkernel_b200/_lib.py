@@ -48,6 +48,9 @@ SIGNATURES = {
     "dgk_ti_connect3d": [_I64, _PI64, _PI64, _PI64],
     "dgk_face_connector": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI64, _PI64],
     "dgk_read_gambit": [C.c_char_p, _PI64, _PD, _PD, _PD, _PI64, _PI64, _PI64],
+    "dgk_halo_plan": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI32, _I32, _I32, _PI64, _PI64, _PI32, _PI64,
+                      _PI64, _PI64, _PI64],
+    "dgk_gather_values": [_P, _I32, _I64, _P, _I64, _P, _P],
     "dgk_face_gather_map": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI32],
     "dgk_init_field_parts": [_P, _S, _S, _S, _S, _D, _I32, _PD],
     "dgk_mlp_param_count": [_I32, _PI64],

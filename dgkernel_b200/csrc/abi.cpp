@@ -258,6 +258,25 @@ int dgk_face_connector(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const
       for (int64_t v : fc.place[i]) place_idx[o++] = v;
   });
 }
+int dgk_halo_plan(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP, const int64_t *EToP,
+                  int32_t npart, const int32_t *part_rank, int32_t nranks, int32_t rank, const int64_t *local_off,
+                  int64_t *counts, int32_t *gmap, int64_t *send_idx, int64_t *send_count, int64_t *recv_count,
+                  int64_t *recv_off) {
+  return guard(nullptr, [&] {
+    if (!vmapP || !EToP || !part_rank || !local_off || !counts) throw dgk::Error(DGK_ERR_INVALID, "halo plan: null argument");
+    const dgk::HaloPlan hp = dgk::halo_plan(K, Nfaces, Nfp, Np, vmapP, EToP, npart, part_rank, nranks, rank, local_off);
+    counts[0] = (int64_t)hp.gmap.size();
+    counts[1] = hp.halo_values;
+    counts[2] = (int64_t)hp.send_idx.size();
+    if (!gmap) return;
+    std::copy(hp.gmap.begin(), hp.gmap.end(), gmap);
+    if (send_idx) std::copy(hp.send_idx.begin(), hp.send_idx.end(), send_idx);
+    if (send_count) std::copy(hp.send_count.begin(), hp.send_count.end(), send_count);
+    if (recv_count) std::copy(hp.recv_count.begin(), hp.recv_count.end(), recv_count);
+    if (recv_off) std::copy(hp.recv_off.begin(), hp.recv_off.end(), recv_off);
+  });
+}
+
 int dgk_face_gather_map(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP,
                         const int64_t *EToP, int32_t npart, const int64_t *node_off, int32_t *gmap) {
   return guard(nullptr, [&] { dgk::face_gather_map(K, Nfaces, Nfp, Np, vmapP, EToP, npart, node_off, gmap); });

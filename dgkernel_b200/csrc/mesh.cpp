@@ -148,6 +148,77 @@ void face_gather_map(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmap
     }
 }
 
+HaloPlan halo_plan(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmapP, const int64_t *EToP, int npart,
+                   const int32_t *part_rank, int nranks, int rank, const int64_t *local_off) {
+  if (nranks < 1 || rank < 0 || rank >= nranks) throw std::invalid_argument("rank outside 0..nranks-1");
+  for (int p = 0; p < npart; ++p)
+    if (part_rank[p] < 0 || part_rank[p] >= nranks) throw std::invalid_argument("partition assigned to no rank");
+  FaceConnector fc = face_connector(K, Nfaces, Nfp, Np, vmapP, EToP, npart);
+  const int P = fc.nparts;
+  const int64_t NF = (int64_t)Nfaces * Nfp;
+  std::vector<int> local;  // this rank's partitions, ascending
+  std::vector<int> lidx((size_t)P, -1);
+  for (int p = 0; p < P; ++p)
+    if (part_rank[p] == rank) {
+      lidx[(size_t)p] = (int)local.size();
+      local.push_back(p);
+    }
+  const int L = (int)local.size();
+  std::vector<int64_t> face_base((size_t)L + 1, 0);  // the rank's P-buffers back to back
+  for (int i = 0; i < L; ++i) face_base[(size_t)i + 1] = face_base[(size_t)i] + fc.elems[(size_t)local[(size_t)i]] * NF;
+  HaloPlan hp;
+  hp.gmap.assign((size_t)face_base[(size_t)L], -1);
+  hp.send_count.assign((size_t)nranks, 0);
+  hp.recv_count.assign((size_t)nranks, 0);
+  hp.recv_off.assign((size_t)nranks, 0);
+  auto put = [&](int64_t pos, int64_t v) {
+    if (v > INT32_MAX) throw std::runtime_error("gather index exceeds int32");
+    hp.gmap[(size_t)pos] = (int32_t)v;
+  };
+  // neighbours in this rank's own partitions
+  for (int i = 0; i < L; ++i) {
+    const int dst = local[(size_t)i];
+    for (int src = 0; src < P; ++src) {
+      if (part_rank[src] != rank) continue;
+      const auto &pk = fc.pick[(size_t)src * P + dst];
+      const auto &pl = fc.place[(size_t)dst * P + src];
+      for (size_t k = 0; k < pk.size(); ++k) put(face_base[(size_t)i] + pl[k], local_off[lidx[(size_t)src]] + pk[k]);
+    }
+  }
+  // received from peer q, in wire order, into the halo
+  int64_t h = 0;
+  for (int q = 0; q < nranks; ++q) {
+    hp.recv_off[(size_t)q] = h;
+    if (q == rank) continue;
+    for (int i = 0; i < L; ++i) {
+      const int dst = local[(size_t)i];
+      for (int src = 0; src < P; ++src) {
+        if (part_rank[src] != q) continue;
+        const auto &pl = fc.place[(size_t)dst * P + src];
+        for (size_t k = 0; k < pl.size(); ++k) put(face_base[(size_t)i] + pl[k], local_off[L] + h++);
+      }
+    }
+    hp.recv_count[(size_t)q] = h - hp.recv_off[(size_t)q];
+  }
+  hp.halo_values = h;
+  // sent to peer q, in the order q receives them
+  for (int q = 0; q < nranks; ++q) {
+    if (q == rank) continue;
+    const int64_t before = (int64_t)hp.send_idx.size();
+    for (int dst = 0; dst < P; ++dst) {
+      if (part_rank[dst] != q) continue;
+      for (int i = 0; i < L; ++i) {
+        const int src = local[(size_t)i];
+        for (int64_t v : fc.pick[(size_t)src * P + dst]) hp.send_idx.push_back(local_off[(size_t)i] + v);
+      }
+    }
+    hp.send_count[(size_t)q] = (int64_t)hp.send_idx.size() - before;
+  }
+  for (int32_t g : hp.gmap)
+    if (g < 0) throw std::runtime_error("halo plan: a face point has no source");
+  return hp;
+}
+
 int64_t slot_padded(int64_t k) { return (k + 31) / 32 * 32; }
 
 CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,

@@ -34,6 +34,20 @@ CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off,
                            const int64_t *slot_prefix, int Np, int Nfp, const int32_t *gmap);
 int64_t slot_padded(int64_t k);  // k rounded up to whole 32-element slots
 
+// Exchange plan of one rank when partitions are spread over ranks (part_rank[p]), built from the FaceConnector
+// pick/place lists (utils/face_connector.go:143-187).  The rank's state array holds its partitions at
+// local_off[0..L-1] (value offsets, ascending partition id) and a halo at local_off[L].  For peer rank q the
+// wire order is: destination partitions of the receiver ascending, source partitions of the sender ascending,
+// pick order within each pair.  gmap covers the rank's face points (packed, partition by partition).
+struct HaloPlan {
+  std::vector<int32_t> gmap;
+  std::vector<int64_t> send_count, recv_count, recv_off;  // per peer rank
+  std::vector<int64_t> send_idx;                          // concatenated over peers, local value indices
+  int64_t halo_values = 0;
+};
+HaloPlan halo_plan(int64_t K, int Nfaces, int Nfp, int Np, const int64_t *vmapP, const int64_t *EToP, int npart,
+                   const int32_t *part_rank, int nranks, int rank, const int64_t *local_off);
+
 // Gambit neutral file (tetrahedra): vertices in file order, EToV as 0-based vertex positions, EToP from the
 // "p<N>" element groups (empty when the file has at most one group), boundary faces (element, 0-based face,
 // boundary-set index).

@@ -134,10 +134,12 @@ std::vector<T> padded_rows(const std::vector<double> &v, int64_t rows, int64_t c
   return out;
 }
 
-// Tile list over partitions: up to te consecutive elements of one partition per tile.
-std::vector<Tile> make_tiles(const Runner &r, const Binding &node, const Binding *face, int te, int np, int nf) {
+// Tile list over partitions: up to te consecutive elements of one partition per tile (the first nparts
+// partitions; all when nparts < 0).
+std::vector<Tile> make_tiles(const Runner &r, const Binding &node, const Binding *face, int te, int np, int nf,
+                             int nparts = -1) {
   std::vector<Tile> t;
-  for (int p = 0; p < r.npart; ++p)
+  for (int p = 0; p < (nparts < 0 ? r.npart : nparts); ++p)
     for (int64_t s = 0; s < r.K[p]; s += te) {
       Tile x;
       x.node_base = node.offsets[p] + s * np;
@@ -218,6 +220,11 @@ struct RhsOp : Op {
     static const char *gn[9] = {"Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz"};
     static const char *fn[4] = {"nx", "ny", "nz", "Fscale"};
     conservative = R.flag("conservative", 0);
+    // halo=1: the last partition holds neighbour values received from other ranks (slab exchange); it is read
+    // through the gather map and never advanced
+    const int halo = R.flag("halo", 0);
+    require(halo == 0 || r.npart >= 2, R.kname + ": halo=1 needs a halo partition after the rank's own");
+    const int tile_parts = r.npart - (halo ? 1 : 0);
     u = R.array("u");
     if (rhs_only) {
       rhs = R.array("rhs");
@@ -265,7 +272,7 @@ struct RhsOp : Op {
     const int te_tma = tma_ok ? dmma_tile_elems(N) : 0;
     use_tma = false;
     if (te_tma > 0) {
-      auto tl = make_tiles(r, *u, face[0], te_tma, (int)np, nf);
+      auto tl = make_tiles(r, *u, face[0], te_tma, (int)np, nf, tile_parts);
       bool aligned = true;
       for (const Tile &x : tl)
         aligned = aligned && (x.node_base * (int64_t)sizeof(T)) % 16 == 0 &&
@@ -277,7 +284,7 @@ struct RhsOp : Op {
       }
     }
     if (!use_tma) {
-      auto tl = make_tiles(r, *u, face[0], tile_elems(N), (int)np, nf);
+      auto tl = make_tiles(r, *u, face[0], tile_elems(N), (int)np, nf, tile_parts);
       ntiles = (int)tl.size();
       tiles.upload(tl.data(), tl.size() * sizeof(Tile));
     }

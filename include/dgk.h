@@ -181,6 +181,22 @@ int dgk_ti_connect3d(int64_t K, const int64_t *EToV, int64_t *EToE, int64_t *ETo
 int dgk_face_connector(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP,
                        const int64_t *EToP, int32_t npart, int64_t *pick_len, int64_t *pick_idx,
                        int64_t *place_idx);
+/* Slab exchange plan of one rank (the FaceConnector pick -> exchange -> place of utils/face_connector.go:143-187
+ * across ranks; partitions/gather_scatter_array_design.md:176-228).  Partition p lives on rank part_rank[p];
+ * the rank's state array holds its partitions at local_off[0..L-1] and a halo at local_off[L].  First call
+ * with gmap == NULL: counts[0] = face points of the rank (gmap length), counts[1] = halo values, counts[2] =
+ * values sent.  Second call: gmap (int32, the rank's face points partition by partition, remote neighbours
+ * pointing into the halo), send_idx (local value indices to pack, peer by peer ascending), and per peer rank
+ * send_count, recv_count, recv_off (offset in the halo).  Wire order for each (sender, receiver): destination
+ * partitions ascending, source partitions ascending, pick order within a pair. */
+int dgk_halo_plan(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, const int64_t *vmapP, const int64_t *EToP,
+                  int32_t npart, const int32_t *part_rank, int32_t nranks, int32_t rank, const int64_t *local_off,
+                  int64_t *counts, int32_t *gmap, int64_t *send_idx, int64_t *send_count, int64_t *recv_count,
+                  int64_t *recv_off);
+/* Pack step of the exchange: dst[i] = src[idx[i]] for i < n, values of dtype (DGK_FLOAT32 / DGK_FLOAT64), all
+ * pointers device memory, on cuda_stream.  An index outside [0, src_count) yields 0 (no read). */
+int dgk_gather_values(const void *src, int32_t dtype, int64_t src_count, const int64_t *idx, int64_t n, void *dst,
+                      void *cuda_stream);
 /* Fused pick->exchange->place gather map: for every face point of partition p (in that partition's
  * P-buffer order), the absolute value index of its neighbour node in an array whose partition p starts
  * at node_off[p].  This is the one-address-space form of the FaceConnector exchange. */
