@@ -19,7 +19,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 INC = ["-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
 CXXFLAGS = ["-O3", "-std=c++17"]
 
-CU = ["kernels.cu", "kernels_tma.cu", "setup.cu", "ops.cu", "noalloc.cu", "mixed.cu", "av.cu", "tcm.cu", "oz.cu", "exchange.cu"]
+CU = ["kernels.cu", "kernels_tma.cu", "setup.cu", "ops.cu", "noalloc.cu", "mixed.cu", "av.cu", "tcm.cu", "oz.cu", "exchange.cu", "lsens.cu"]
 CPP = ["runner.cpp", "element.cpp", "mesh.cpp", "gambit.cpp", "abi.cpp"]
 
 

@@ -143,6 +143,11 @@ class _TetBurgers:
             params += [Temp(nm).Type(Float32).Size(K * Np).Align(WarpAlign)
                        for nm in ("uhi", "ulo", "uhiNext", "uloNext", "resu")]
             params += [Input(f"Bary_{sn}").Bind(bary_matrix(el)).ToMatrix().Static()]
+        if getattr(self, "learned", None):
+            if not self.mixed:
+                raise ValueError("the learned-sensor viscosity runs on the mixed stage (dtype MIXED, mma=True)")
+            params += [Input(f"Vinv_{sn}").Bind(el.Vinv).ToMatrix().Static()]
+            params += [Input("MLP").Bind(np.zeros((1, mlp_param_count(Np)))).ToMatrix().DeviceMemType(Float32)]
         if self.visc:
             if self.mixed or self.dtype != np.float64:
                 raise ValueError("the artificial-viscosity stage runs in float64")
@@ -186,12 +191,15 @@ class _TetBurgers:
         self.conservative = conservative
         self.u0 = self.get("u")
         self.dt = cfl * self.hmin / float(np.max(np.abs(self.u0)))
-        if self.visc:
+        if self.visc or getattr(self, "learned", None):
             self.av = {"eps0": eps0, "c0": c0, "kappa": kappa, "lo": conf[0], "hi": conf[1]}
             fs = self.get("Fscale").reshape(self.K, -1)
             self.eps_max = eps0 * float(np.max(2.0 / fs.max(axis=1))) / self.N
             if self.eps_max > 0:  # diffusive limit of the explicit step
                 self.dt = min(self.dt, cfl * self.hmin ** 2 / self.eps_max)
+        if getattr(self, "learned", None):
+            fixed += [f"Vinv_{self.el.ShortName}", "MLP"]
+        if self.visc:
             sn = self.el.ShortName
             fixed += ["eps", "qx", "qy", "qz", f"Vinv_{sn}", "MLP"]
             feats = ["u", *GEO, *FACE, "gmap", *fixed_m, f"Vinv_{sn}", "MLP", "feat", "sigma", "mlpSigma"]
@@ -216,6 +224,8 @@ class _TetBurgers:
             args.append(f"tensor={int(self.tensor)}")
         if getattr(self, "mma", None):
             args.append("mma=1")
+        if getattr(self, "learned", None):
+            args.append(self._av_args(self.learned))
         if warps:
             args.append(f"warps={warps}")
         if ring:
@@ -231,13 +241,16 @@ class _TetBurgers:
         self.runner.BuildKernel(self.op_id(warps, ring), "rhsStage")
 
     def set_sensor(self, sensor: str, params=None):
-        """Viscosity stage: switch the sensor ("none", "pp" or "mlp"; for "mlp" the network's float32
-        parameters) and rebuild the stage."""
-        if not self.visc:
+        """Viscosity stage (or the learned-sensor mixed stage): switch the sensor ("none", "pp", "mlp"; "mlp0" on
+        the mixed stage; for the network sensors its float32 parameters) and rebuild the stage."""
+        if not (self.visc or getattr(self, "learned", None)):
             raise ValueError("problem built without viscosity")
         if params is not None:
             self.runner.CopyToDevice("MLP", np.asarray(params, dtype=np.float64).reshape(1, -1))
-        self.visc = sensor
+        if self.visc:
+            self.visc = sensor
+        else:
+            self.learned = sensor
         self.build_stage()
 
     def sensor_features(self, sensor: str = "pp"):
@@ -321,8 +334,10 @@ class BurgersProblem(_TetBurgers):
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
                  cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None,
                  viscosity=None, eps0: float = 1.0, c0: float = 0.0, kappa: float = 1.0, conf=(0.1, 0.9),
-                 mode_sigma: float = 0.1, tensor=None, mma=None, derivatives=False):
+                 mode_sigma: float = 0.1, tensor=None, mma=None, derivatives=False, learned=None):
         self.n, self.nslab = n, nslab
+        # mixed tensor-core stage with learned-sensor (or PP) artificial viscosity: "pp", "mlp" or "mlp0"
+        self.learned = learned
         self.derivatives = derivatives  # also bind DuDx, DuDy, DuDz for the `differentiate` operator
         self.tensor = tensor  # mixed form: None = by order (tensor cores for orders 6, 7), True / False to force
         self.mma = mma  # mixed form, orders 1..4: element-local products on the tensor cores (3-part BF16)

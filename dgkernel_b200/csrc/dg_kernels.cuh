@@ -114,6 +114,8 @@ struct MixedArgs {
   const float *Dm;               // [NP][NPJ][3]: Dr, Ds, Dt entries interleaved per column, zero-padded
   const float *lift;             // [NP][4 Nfp]
   const unsigned char *bmat;     // tensor-core form: split BF16 operands of D and LIFT (tcm_pack_operands)
+  const int32_t *vslot;          // tensor-core form with viscosity: per element slot, row of visc or -1
+  const double *visc;            // [row][Np] viscous right-hand side added before the update
   const double *bary;            // [NP][3] barycentric weights of vertices B, C, D at each node
   const int32_t *vtx;            // node index of vertices A, B, C, D
   const uint8_t *ftab;           // [ncodes][Nfp] neighbour-local node index of each face point
@@ -163,6 +165,39 @@ struct OzArgs {
   const int32_t *fmask;         // [4 Nfp]
   int ncodes;
   double a, b, dt;
+  int *status;
+};
+
+// ---- learned-sensor viscosity on the mixed stage (lsens.cu) ----
+struct LsArgs {
+  const MTile *tiles;  // the mixed stage's tiles (element slots)
+  int ntiles;
+  int npart;
+  const int64_t *slot_prefix;  // device, npart + 1: first element slot of each partition
+  const int64_t *kpart;        // device, npart: elements per partition
+  const int64_t *uoff;         // device, npart: value offset of each partition in the state arrays
+  const int64_t *goff;         // device, npart: value offset in the FP64 metric arrays
+  const int64_t *foff;         // device, npart: value offset in the face arrays and the gather map
+  const float *uhi, *ulo;      // the state this stage reads
+  const double *geo[9];        // rx .. tz per node (FP64)
+  const double *face[4];       // nx, ny, nz, Fscale per face point (FP64)
+  const int32_t *gmap;         // absolute neighbour value index per face point
+  const int32_t *conn;         // compact connectivity per element slot (neighbour base per face)
+  int64_t n_u_values;
+  const double *Dr, *Ds, *Dt, *Vinv, *LIFT;  // row-major
+  const int32_t *fmask, *top;
+  const double *h_over_n;      // per element slot
+  int mode;                    // 1 PP, 2 MLP with PP fallback, 3 as 2 with outputs <= lo read as smooth
+  double eps0, s0, kappa;
+  float conf_lo, conf_hi;
+  const unsigned short *mlp16;
+  double *eps;                 // per element slot
+  int32_t *aslot;              // per element slot: index in the active list or -1
+  int32_t *alist, *tflag, *vslot, *tlist;
+  int32_t *counts;             // [0] active, [1] touched, [2] network fallbacks to PP
+  double *eq;                  // [active][3][Np]: eps q
+  double *visc;                // [touched][Np]: the viscous right-hand side
+  int64_t nslots;
   int *status;
 };
 

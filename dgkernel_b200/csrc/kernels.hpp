@@ -59,6 +59,11 @@ void oz_pack_operands(int N, const double *Dr, const double *Ds, const double *D
 void prepare_rhs_oz(int N);  // attributes, before any stream capture
 bool launch_rhs_oz(int N, const OzArgs &A, int conservative, int num_sms, cudaStream_t st, LaunchInfo *info);
 
+// Learned-sensor viscosity on the tensor-core mixed stage (lsens.cu), orders 1..4.
+bool ls_supported(int N);
+void prepare_ls(int N);  // attributes, before any stream capture
+void launch_ls(int N, const LsArgs &A, int num_sms, cudaStream_t st);
+
 // Artificial-viscosity stage and the sensor MLP (av.cu).
 void launch_av(int N, const AvArgs &A, int num_sms, cudaStream_t st);
 int mlp_param_count(int nin);

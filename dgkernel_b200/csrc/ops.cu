@@ -392,6 +392,14 @@ struct MixedOp : Op {
   int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0, tensor = 0, mma = 0;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
   DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat, rexp, bmat;
+  // learned-sensor viscosity (sensor=pp|mlp|mlp0 with mma=1)
+  int lmode = 0;
+  double eps0 = 1.0, s0 = 0.0, kappa = 1.0;
+  float conf_lo = 0.1f, conf_hi = 0.9f;
+  int64_t l_nslots = 0;
+  Binding *geoB[9] = {}, *faceB[4] = {}, *gmapB = nullptr, *mlpB = nullptr;
+  DevBuf l_dr, l_ds, l_dt, l_vinv, l_lift, l_top, l_hon, l_mlp16, l_sp, l_kp, l_uo, l_go, l_fo, l_eps, l_aslot, l_alist,
+      l_tflag, l_vslot, l_tlist, l_counts, l_eq, l_visc;
   LaunchInfo info;
 
   template <typename G>
@@ -563,9 +571,130 @@ struct MixedOp : Op {
       }
     ntiles = (int)tl.size();
     tiles.upload(tl.data(), std::max<size_t>(tl.size(), 1) * sizeof(MTile));
+    const std::string sensor = lower(R.word("sensor", "none"));
+    if (sensor != "none") {
+      if (sensor == "pp") lmode = 1;
+      else if (sensor == "mlp") lmode = 2;
+      else if (sensor == "mlp0") lmode = 3;
+      else throw Error(DGK_ERR_INVALID, R.kname + ": sensor must be none, pp, mlp or mlp0");
+      require(mma && ls_supported(N), R.kname + ": the learned-sensor viscosity runs on the tensor-core mixed stage "
+                                               "(mma=1, orders 1..4)");
+      require(geo[0]->dev_dtype == DGK_FLOAT64 && face[0]->dev_dtype == DGK_FLOAT64,
+              R.kname + ": the viscous term reads float64 metric and face arrays");
+      eps0 = R.num("eps0", 1.0);
+      kappa = R.num("kappa", 1.0);
+      conf_lo = (float)R.num("lo", 0.1);
+      conf_hi = (float)R.num("hi", 0.9);
+      require(kappa > 0.0 && eps0 >= 0.0, R.kname + ": kappa > 0 and eps0 >= 0");
+      s0 = -(R.num("c0", 0.0) + 4.0 * std::log10((double)N));
+      for (int i = 0; i < 9; ++i) geoB[i] = geo[i];
+      for (int i = 0; i < 4; ++i) faceB[i] = face[i];
+      gmapB = gmap;
+      Binding *Vi = R.matrix("Vinv");
+      require(Vi->rows == np && Vi->cols == np, R.kname + ": Vinv must be Np x Np");
+      auto rm = [&](const std::vector<double> &m, DevBuf &d) { d.upload(m.data(), m.size() * sizeof(double)); };
+      rm(Dr->mat, l_dr);
+      rm(Ds->mat, l_ds);
+      rm(Dt->mat, l_dt);
+      rm(Vi->mat, l_vinv);
+      rm(L->mat, l_lift);
+      if (lmode >= 2) {
+        mlpB = R.matrix("MLP");
+        require(mlpB->rows * mlpB->cols == mlp_param_count((int)np) && mlpB->dev_dtype == DGK_FLOAT32,
+                R.kname + ": MLP must hold " + std::to_string(mlp_param_count((int)np)) + " float32 parameters");
+        l_mlp16.alloc(sizeof(uint16_t) * ((size_t)mlp_param_count((int)np) + 8));
+      }
+      std::vector<int32_t> tp;
+      for (int i = 0; i <= N; ++i)  // modes ordered i, j, k (vandermonde3d.go:15-42)
+        for (int j = 0; j <= N - i; ++j)
+          for (int k = 0; k <= N - i - j; ++k) tp.push_back(i + j + k == N ? 1 : 0);
+      l_top.upload(tp.data(), tp.size() * sizeof(int32_t));
+      // h_e / N per element slot, h_e = 2 / max Fscale over the element's face points
+      l_nslots = slot_prefix[P];
+      std::vector<double> fs((size_t)face[3]->offsets.back());
+      cuda_check(cudaMemcpy(fs.data(), face[3]->dptr, fs.size() * sizeof(double), cudaMemcpyDeviceToHost), "Fscale");
+      std::vector<double> h((size_t)std::max<int64_t>(l_nslots, 1), 0.0);
+      for (int p = 0; p < P; ++p)
+        for (int64_t e = 0; e < r.K[p]; ++e) {
+          double m = 0.0;
+          for (int k = 0; k < nf; ++k) m = std::max(m, fs[(size_t)(face[3]->offsets[p] + e * nf + k)]);
+          require(m > 0.0, R.kname + ": Fscale must be positive");
+          h[(size_t)(slot_prefix[p] + e)] = 2.0 / m / N;
+        }
+      l_hon.upload(h.data(), h.size() * sizeof(double));
+      std::vector<int64_t> kp(r.K.begin(), r.K.end()), uo(uhi->offsets.begin(), uhi->offsets.begin() + P),
+          go(geo[0]->offsets.begin(), geo[0]->offsets.begin() + P), fo(face[0]->offsets.begin(), face[0]->offsets.begin() + P);
+      l_sp.upload(slot_prefix.data(), slot_prefix.size() * sizeof(int64_t));
+      l_kp.upload(kp.data(), kp.size() * sizeof(int64_t));
+      l_uo.upload(uo.data(), uo.size() * sizeof(int64_t));
+      l_go.upload(go.data(), go.size() * sizeof(int64_t));
+      l_fo.upload(fo.data(), fo.size() * sizeof(int64_t));
+      const size_t ns = (size_t)std::max<int64_t>(l_nslots, 1);
+      l_eps.alloc(ns * sizeof(double));
+      std::vector<int32_t> minus((size_t)ns, -1), zero((size_t)ns, 0);
+      l_aslot.upload(minus.data(), ns * sizeof(int32_t));
+      l_vslot.upload(minus.data(), ns * sizeof(int32_t));
+      l_tflag.upload(zero.data(), ns * sizeof(int32_t));
+      l_alist.alloc(ns * sizeof(int32_t));
+      l_tlist.alloc(ns * sizeof(int32_t));
+      l_counts.alloc(4 * sizeof(int32_t));
+      l_eq.alloc(ns * 3 * (size_t)np * sizeof(double));  // capacity: every element active
+      l_visc.alloc(ns * (size_t)np * sizeof(double));
+    }
+  }
+  // Learned-sensor viscosity of the current state: sensor, active and touched lists, BR1 gradient and
+  // divergence on the GPU; the tensor-core stage then adds the viscous right-hand side.
+  void launch_viscosity(Runner &r) {
+    LsArgs L{};
+    L.tiles = tiles.get<MTile>();
+    L.ntiles = ntiles;
+    L.npart = r.npart;
+    L.slot_prefix = l_sp.get<int64_t>();
+    L.kpart = l_kp.get<int64_t>();
+    L.uoff = l_uo.get<int64_t>();
+    L.goff = l_go.get<int64_t>();
+    L.foff = l_fo.get<int64_t>();
+    L.uhi = reinterpret_cast<const float *>(uhi->dptr);
+    L.ulo = reinterpret_cast<const float *>(ulo->dptr);
+    for (int i = 0; i < 9; ++i) L.geo[i] = reinterpret_cast<const double *>(geoB[i]->dptr);
+    for (int i = 0; i < 4; ++i) L.face[i] = reinterpret_cast<const double *>(faceB[i]->dptr);
+    L.gmap = reinterpret_cast<const int32_t *>(gmapB->dptr);
+    L.conn = conn.get<int32_t>();
+    L.n_u_values = uhi->offsets.back();
+    L.Dr = l_dr.get<double>();
+    L.Ds = l_ds.get<double>();
+    L.Dt = l_dt.get<double>();
+    L.Vinv = l_vinv.get<double>();
+    L.LIFT = l_lift.get<double>();
+    L.fmask = fmask.get<int32_t>();
+    L.top = l_top.get<int32_t>();
+    L.h_over_n = l_hon.get<double>();
+    L.mode = lmode;
+    L.eps0 = eps0;
+    L.s0 = s0;
+    L.kappa = kappa;
+    L.conf_lo = conf_lo;
+    L.conf_hi = conf_hi;
+    if (lmode >= 2) {
+      launch_to_half(reinterpret_cast<const float *>(mlpB->dptr), l_mlp16.p, mlp_param_count((N + 1) * (N + 2) * (N + 3) / 6), r.stream());
+      L.mlp16 = l_mlp16.get<unsigned short>();
+    }
+    L.eps = l_eps.get<double>();
+    L.aslot = l_aslot.get<int32_t>();
+    L.alist = l_alist.get<int32_t>();
+    L.tflag = l_tflag.get<int32_t>();
+    L.vslot = l_vslot.get<int32_t>();
+    L.tlist = l_tlist.get<int32_t>();
+    L.counts = l_counts.get<int32_t>();
+    L.eq = l_eq.get<double>();
+    L.visc = l_visc.get<double>();
+    L.nslots = l_nslots;
+    L.status = r.status_word();
+    launch_ls(N, L, r.num_sms, r.stream());
   }
   std::vector<std::string> scalar_names() const override { return {"a", "b", "dt"}; }
   void prepare(Runner &) override {
+    if (lmode) prepare_ls(N);
     if (mma)
       prepare_rhs_tcm(N, warps);
     else if (tensor)
@@ -629,6 +758,11 @@ struct MixedOp : Op {
     A.status = r.status_word();
     if (mma) {
       A.bmat = bmat.get<unsigned char>();
+      if (lmode) {
+        launch_viscosity(r);
+        A.vslot = l_vslot.get<int32_t>();
+        A.visc = l_visc.get<double>();
+      }
       if (!launch_rhs_tcm(N, A, warps, r.num_sms, r.stream(), &info))
         throw Error(DGK_ERR_UNSUPPORTED, "tensor-core mixed stage: shared memory does not fit this order");
       std::swap(uhi->dptr, uhin->dptr);

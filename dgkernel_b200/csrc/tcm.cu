@@ -476,6 +476,8 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
+      // the learned-sensor viscosity: this element's row of viscous right-hand side, if it has one
+      const int vrow = (A.vslot && valid) ? A.vslot[tl.elem_slot + e] : -1;
       if (ldone) {
 #pragma unroll
         for (int cc = 0; cc < NCE; ++cc) {
@@ -488,7 +490,8 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
               const int i = 8 * c + q;
               if (i < NP && valid) {
                 const int o = e * NP + i;
-                const float rn = fmaf(dt, lf[q], t0[cc][q]);
+                float rn = fmaf(dt, lf[q], t0[cc][q]);
+                if (vrow >= 0) rn = fmaf(dt, (float)A.visc[(int64_t)vrow * NP + i], rn);
                 float hn, ln;
                 stage_update(hi[i], lo[i], rn, bh, bl, hn, ln);
                 sHi[o] = hn;

@@ -293,8 +293,9 @@ int ora_max_threads(void)
  * simplex3dp.go:15-36, order i, j, k of vandermonde3d.go:15-42); S = log10(sum over modes of total degree N
  * of uhat^2 / sum over all modes of uhat^2); activation sigma = 0 for S < s0 - kappa, 1 for S > s0 + kappa,
  * else (1 + sin(pi (S - s0) / (2 kappa))) / 2.  Viscosity eps_e = eps0 sigma_e h_e / N with h_e = 2 / max
- * of the element's Fscale.  Learned mode: sigma = MLP(uhat / |uhat|) (nin -> 32 -> 32 -> 1, tanh, tanh,
- * sigmoid) where the MLP output lies outside (conf_lo, conf_hi), the PP sigma inside that band.
+ * of the element's Fscale.  Learned mode (2): sigma = MLP(uhat / |uhat|) (nin -> 32 -> 32 -> 1, tanh, tanh,
+ * sigmoid) where the MLP output lies outside (conf_lo, conf_hi), the PP sigma inside that band; mode 3 is the
+ * same with outputs at or below conf_lo read as a smooth element, sigma = 0.
  *
  * Viscous term (BR1, central fluxes): q_d = D_d u + LIFT (Fscale n_d (uP - uM) / 2), d = x, y, z; then
  * rhs += eps_e sum_d D_d q_d + LIFT (Fscale 1/2 sum_d n_d (epsP qP_d - epsM qM_d)). */
@@ -376,9 +377,10 @@ void ora_rhs_av(int Np, int Nfp, int N, const double *Dr, const double *Ds, cons
         modal_features(Np, Vinv, top, ue, uh, &S, ft);
         if (mode == 1) {
             sig = pp_sigma(S, s0, kappa);
-        } else if (mode == 2) {
+        } else if (mode == 2 || mode == 3) {
             sig = ora_mlp_forward1(Np, mlp, ft);
             if (sig > conf_lo && sig < conf_hi) sig = pp_sigma(S, s0, kappa);
+            else if (mode == 3 && sig <= conf_lo) sig = 0.0;
         }
         double fmax = 0.0;
         for (int m = 0; m < NF; ++m) fmax = fmax > Fscale[e * NF + m] ? fmax : Fscale[e * NF + m];

@@ -153,7 +153,7 @@ class AVState:
     """Artificial-viscosity oracle on one packed mesh (all partitions contiguous; neighbour traces through
     the global VmapP)."""
 
-    MODES = {"none": 0, "pp": 1, "mlp": 2}
+    MODES = {"none": 0, "pp": 1, "mlp": 2, "mlp0": 3}  # mlp0: network outputs <= lo are smooth (eps = 0)
 
     def __init__(self, prob, eps0=1.0, c0=0.0, kappa=1.0, conf=(0.1, 0.9)):
         el, geo = prob.el, prob.geo

@@ -1,0 +1,79 @@
+"""Learned-sensor viscosity on the tensor-core mixed stage (rhsStageMixed with mma=1 and sensor=pp|mlp|mlp0):
+the sensor over every element, the BR1 viscous term only on the elements where it is not zero, the inviscid
+part in the mixed form (compensated FP32 state, three-part BF16 tensor-core products), through the runner.
+
+Bounds, relative L2 against the FP64 oracle's viscosity stage (ora_run_av) after 10 LSERK4 stages of an
+under-resolved random-mode field on which the sensor is active: PP sensor 1e-7 (the mixed form's bound; the
+viscous term runs in FP64; measured 5.3e-8); network sensors 1.2e-7, twice the measured 5.4e-8 / 5.6e-8 (FP32
+network sums against the oracle's FP64 sums, weights rounded to FP16 on both sides).  With eps0 = 0 the stage equals the mixed
+tensor-core stage bit for bit; with the sensor on it must differ from it by far more than the bound.
+"""
+import numpy as np
+import pytest
+
+from dgkernel_b200 import sensor as SN
+from dgkernel_b200.burgers import BurgersProblem, MIXED
+from oracle import burgers_ref as b
+from oracle import mlp_ref as MR
+from oracle import oracle as O
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _rough(sensor="pp", n=4, nslab=2, **kw):
+    return BurgersProblem(4, n, nslab, MIXED, "modes", mode_sigma=0.3, mma=True, learned=sensor, **kw)
+
+
+def _oracle(u0, dt, nst, mode, mlp=None, n=4):
+    u = np.ascontiguousarray(u0, dtype=np.float64).copy()
+    resu = np.zeros_like(u)
+    O.AVState(b.Problem(4, n, 1, "sine")).run(u, resu, dt, nst, mode, mlp=mlp)
+    return u
+
+
+def test_learned_stage_pp_matches_oracle():
+    P = _rough("pp")
+    u0 = P.u0.copy()
+    P.run_stages(10)
+    got = P.get("u")
+    want = _oracle(u0, P.dt, 10, "pp")
+    err = rel_l2(got, want)
+    # the viscosity acts: the inviscid mixed stage lands far from the oracle's viscous run
+    Q = BurgersProblem(4, 4, 2, MIXED, "modes", mode_sigma=0.3, mma=True)
+    Q.dt = P.dt
+    Q.build_stage()
+    Q.run_stages(10)
+    gap = rel_l2(Q.get("u"), want)
+    print(f"PP sensor: relative L2 vs oracle {err:.3e}; inviscid stage vs oracle {gap:.3e}")
+    assert err < 1e-7 and gap > 100 * err, (err, gap)
+    P.free()
+    Q.free()
+
+
+def test_learned_stage_without_viscosity_is_the_mixed_stage():
+    A = _rough("pp", eps0=0.0)
+    B = BurgersProblem(4, 4, 2, MIXED, "modes", mode_sigma=0.3, mma=True)
+    B.dt = A.dt
+    B.build_stage()
+    A.run_stages(10)
+    B.run_stages(10)
+    assert np.array_equal(A.get("uhi"), B.get("uhi")) and np.array_equal(A.get("ulo"), B.get("ulo"))
+    A.free()
+    B.free()
+
+
+@pytest.mark.parametrize("sensor", ["mlp", "mlp0"])
+def test_learned_stage_network_matches_oracle(sensor):
+    rng = np.random.default_rng(4)
+    p = (SN.init_params(35, seed=5) * 3 + rng.normal(size=2241).astype(np.float32) * 0.1).astype(np.float32)
+    P = _rough(sensor)
+    P.set_sensor(sensor, p)
+    u0 = P.u0.copy()
+    P.run_stages(10)
+    want = _oracle(u0, P.dt, 10, sensor, mlp=MR.to_fp16(p))
+    err = rel_l2(P.get("u"), want)
+    print(f"{sensor}: relative L2 vs oracle {err:.3e}")
+    assert err < 1.2e-7, err
+    P.free()
