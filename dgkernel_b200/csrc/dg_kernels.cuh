@@ -184,7 +184,8 @@ struct LsArgs {
   const int32_t *gmap;         // absolute neighbour value index per face point
   const int32_t *conn;         // compact connectivity per element slot (neighbour base per face)
   int64_t n_u_values;
-  const double *Dr, *Ds, *Dt, *Vinv, *LIFT;  // row-major
+  const double *Dr, *Ds, *Dt, *LIFT;  // transposed: [j][i] (LIFT [m][i])
+  const double *Vinv;                  // row-major [i][j]
   const int32_t *fmask, *top;
   const double *h_over_n;      // per element slot
   int mode;                    // 1 PP, 2 MLP with PP fallback, 3 as 2 with outputs <= lo read as smooth

@@ -28,7 +28,6 @@ namespace {
 
 constexpr int kLsHid = 32;
 constexpr int kLsElems = 64;   // sensor pass: elements per block, 4 threads each
-constexpr int kLsThreads = 64; // sparse passes: threads per element (Np, 4 Nfp <= 64 at orders <= 4)
 
 __host__ __device__ constexpr int ls_mlp_params(int nin) {
   return kLsHid * nin + kLsHid + kLsHid * kLsHid + kLsHid + kLsHid + 1;
@@ -198,93 +197,83 @@ __global__ void ls_compact_kernel(const LsArgs A) {
   }
 }
 
-// shared layout of the sparse passes: Dr, Ds, Dt [NP][NP], LIFT [NP][NF], then per-element work buffers
-template <int N>
-__device__ __forceinline__ void load_mats(const LsArgs &A, double *sD, double *sL) {
-  using O = Order<N>;
-  constexpr int NP = O::NP, NF = O::NF;
-  for (int x = threadIdx.x; x < NP * NP; x += blockDim.x) {
-    sD[x] = A.Dr[x];
-    sD[NP * NP + x] = A.Ds[x];
-    sD[2 * NP * NP + x] = A.Dt[x];
-  }
-  for (int x = threadIdx.x; x < NP * NF; x += blockDim.x) sL[x] = A.LIFT[x];
-}
+// Sparse passes: one warp per element, lanes over the element's nodes (i = lane, lane + 32) and face points; the
+// FP64 matrices are read transposed from global memory (DT[j][i], LT[m][i]: a warp's lanes read consecutive
+// values, and the few tens of KB stay in L1), per-warp values in shared memory, no block barrier.
+constexpr int kLsWarps = 8;  // warps (elements in flight) per block
 
 template <int N>
-__global__ void __launch_bounds__(kLsThreads) ls_grad_kernel(const LsArgs A) {
+__global__ void __launch_bounds__(32 * kLsWarps) ls_grad_kernel(const LsArgs A) {
   using O = Order<N>;
   constexpr int NP = O::NP, NF = O::NF;
-  extern __shared__ __align__(16) unsigned char sm[];
-  double *sD = reinterpret_cast<double *>(sm), *sL = sD + 3 * NP * NP;
-  double *su = sL + NP * NF, *sj = su + NP;  // u [NP], n_d Fscale (uP - uM) / 2 [3][NF]
-  load_mats<N>(A, sD, sL);
-  __syncthreads();
-  const int tid = threadIdx.x;
+  __shared__ double s_u[kLsWarps][NP], s_j[kLsWarps][3][NF];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double *su = s_u[w];
   const int n = *reinterpret_cast<volatile const int *>(&A.counts[0]);
-  for (int a = blockIdx.x; a < n; a += gridDim.x) {
+  for (int a = blockIdx.x * kLsWarps + w; a < n; a += gridDim.x * kLsWarps) {
     const int64_t slot = A.alist[a];
     const int p = part_of_slot(A, slot);
     const int64_t le = slot - A.slot_prefix[p];
     const int64_t ub = A.uoff[p] + le * NP, gb = A.goff[p] + le * NP, fb = A.foff[p] + le * NF;
-    if (tid < NP) su[tid] = (double)A.uhi[ub + tid] + (double)A.ulo[ub + tid];
-    __syncthreads();
-    if (tid < NF) {
-      const int32_t g = A.gmap[fb + tid];
-      const double uM = su[A.fmask[tid]];
+    for (int i = lane; i < NP; i += 32) su[i] = (double)A.uhi[ub + i] + (double)A.ulo[ub + i];
+    __syncwarp();
+    for (int m = lane; m < NF; m += 32) {
+      const int32_t g = A.gmap[fb + m];
+      const double uM = su[A.fmask[m]];
       double uP = uM;
       if ((uint64_t)(int64_t)g < (uint64_t)A.n_u_values) {
         uP = (double)A.uhi[g] + (double)A.ulo[g];
       } else {
         atomicExch(A.status, kStatusBadGather);
       }
-      const double jump = 0.5 * (uP - uM) * A.face[3][fb + tid];
-      for (int d = 0; d < 3; ++d) sj[d * NF + tid] = A.face[d][fb + tid] * jump;
+      const double jump = 0.5 * (uP - uM) * A.face[3][fb + m];
+      for (int d = 0; d < 3; ++d) s_j[w][d][m] = A.face[d][fb + m] * jump;
     }
-    __syncthreads();
-    if (tid < NP) {
+    __syncwarp();
+    const double eps = A.eps[slot];
+    for (int i = lane; i < NP; i += 32) {
       double ur = 0.0, us = 0.0, ut = 0.0;
 #pragma unroll 5
       for (int j = 0; j < NP; ++j) {
-        ur = fma(sD[tid * NP + j], su[j], ur);
-        us = fma(sD[NP * NP + tid * NP + j], su[j], us);
-        ut = fma(sD[2 * NP * NP + tid * NP + j], su[j], ut);
+        const double v = su[j];
+        ur = fma(__ldg(A.Dr + j * NP + i), v, ur);
+        us = fma(__ldg(A.Ds + j * NP + i), v, us);
+        ut = fma(__ldg(A.Dt + j * NP + i), v, ut);
       }
-      const double eps = A.eps[slot];
-      for (int d = 0; d < 3; ++d) {
-        double q = A.geo[d][gb + tid] * ur + A.geo[3 + d][gb + tid] * us + A.geo[6 + d][gb + tid] * ut;
+      double q[3];
+      for (int d = 0; d < 3; ++d) q[d] = A.geo[d][gb + i] * ur + A.geo[3 + d][gb + i] * us + A.geo[6 + d][gb + i] * ut;
 #pragma unroll 6
-        for (int m = 0; m < NF; ++m) q = fma(sL[tid * NF + m], sj[d * NF + m], q);
-        A.eq[((int64_t)a * 3 + d) * NP + tid] = eps * q;
+      for (int m = 0; m < NF; ++m) {
+        const double l = __ldg(A.LIFT + m * NP + i);
+        q[0] = fma(l, s_j[w][0][m], q[0]);
+        q[1] = fma(l, s_j[w][1][m], q[1]);
+        q[2] = fma(l, s_j[w][2][m], q[2]);
       }
+      for (int d = 0; d < 3; ++d) A.eq[((int64_t)a * 3 + d) * NP + i] = eps * q[d];
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
 template <int N>
-__global__ void __launch_bounds__(kLsThreads) ls_div_kernel(const LsArgs A) {
+__global__ void __launch_bounds__(32 * kLsWarps) ls_div_kernel(const LsArgs A) {
   using O = Order<N>;
   constexpr int NP = O::NP, NF = O::NF;
-  extern __shared__ __align__(16) unsigned char sm[];
-  double *sD = reinterpret_cast<double *>(sm), *sL = sD + 3 * NP * NP;
-  double *sq = sL + NP * NF, *sfl = sq + 3 * NP;  // eps q [3][NP] of the element, flux [NF]
-  load_mats<N>(A, sD, sL);
-  __syncthreads();
-  const int tid = threadIdx.x;
+  __shared__ double s_q[kLsWarps][3][NP], s_f[kLsWarps][NF];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int n = *reinterpret_cast<volatile const int *>(&A.counts[1]);
-  for (int r = blockIdx.x; r < n; r += gridDim.x) {
+  for (int r = blockIdx.x * kLsWarps + w; r < n; r += gridDim.x * kLsWarps) {
     const int64_t slot = A.tlist[r];
     const int p = part_of_slot(A, slot);
     const int64_t le = slot - A.slot_prefix[p];
     const int64_t gb = A.goff[p] + le * NP, fb = A.foff[p] + le * NF;
     const int a = A.aslot[slot];
-    if (tid < NP)
-      for (int d = 0; d < 3; ++d) sq[d * NP + tid] = a >= 0 ? A.eq[((int64_t)a * 3 + d) * NP + tid] : 0.0;
-    __syncthreads();
-    if (tid < NF) {
-      const int32_t g = A.gmap[fb + tid];
-      const int jM = A.fmask[tid];
+    for (int i = lane; i < NP; i += 32)
+      for (int d = 0; d < 3; ++d) s_q[w][d][i] = a >= 0 ? A.eq[((int64_t)a * 3 + d) * NP + i] : 0.0;
+    __syncwarp();
+    for (int m = lane; m < NF; m += 32) {
+      const int32_t g = A.gmap[fb + m];
+      const int jM = A.fmask[m];
       double ePq[3] = {0.0, 0.0, 0.0};
       int node;
       const int64_t ns = ((uint64_t)(int64_t)g < (uint64_t)A.n_u_values) ? slot_of_value(A, g, NP, &node) : -1;
@@ -296,30 +285,34 @@ __global__ void __launch_bounds__(kLsThreads) ls_div_kernel(const LsArgs A) {
         atomicExch(A.status, kStatusBadGather);
       }
       double v = 0.0;
-      for (int d = 0; d < 3; ++d) v += A.face[d][fb + tid] * (ePq[d] - sq[d * NP + jM]);
-      sfl[tid] = 0.5 * A.face[3][fb + tid] * v;
+      for (int d = 0; d < 3; ++d) v += A.face[d][fb + m] * (ePq[d] - s_q[w][d][jM]);
+      s_f[w][m] = 0.5 * A.face[3][fb + m] * v;
     }
-    __syncthreads();
-    if (tid < NP) {
+    __syncwarp();
+    for (int i = lane; i < NP; i += 32) {
       double div = 0.0;
-      if (a >= 0)
-        for (int d = 0; d < 3; ++d) {
-          const double *qd = sq + d * NP;
-          double qr = 0.0, qs = 0.0, qt = 0.0;
+      if (a >= 0) {
+        double qr[3] = {0.0, 0.0, 0.0}, qs[3] = {0.0, 0.0, 0.0}, qt[3] = {0.0, 0.0, 0.0};
 #pragma unroll 5
-          for (int j = 0; j < NP; ++j) {
-            qr = fma(sD[tid * NP + j], qd[j], qr);
-            qs = fma(sD[NP * NP + tid * NP + j], qd[j], qs);
-            qt = fma(sD[2 * NP * NP + tid * NP + j], qd[j], qt);
+        for (int j = 0; j < NP; ++j) {
+          const double dr = __ldg(A.Dr + j * NP + i), ds = __ldg(A.Ds + j * NP + i), dt = __ldg(A.Dt + j * NP + i);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double v = s_q[w][d][j];
+            qr[d] = fma(dr, v, qr[d]);
+            qs[d] = fma(ds, v, qs[d]);
+            qt[d] = fma(dt, v, qt[d]);
           }
-          div += A.geo[d][gb + tid] * qr + A.geo[3 + d][gb + tid] * qs + A.geo[6 + d][gb + tid] * qt;
         }
+        for (int d = 0; d < 3; ++d)
+          div += A.geo[d][gb + i] * qr[d] + A.geo[3 + d][gb + i] * qs[d] + A.geo[6 + d][gb + i] * qt[d];
+      }
       double lift = 0.0;
 #pragma unroll 6
-      for (int m = 0; m < NF; ++m) lift = fma(sL[tid * NF + m], sfl[m], lift);
-      A.visc[(int64_t)r * NP + tid] = div + lift;
+      for (int m = 0; m < NF; ++m) lift = fma(__ldg(A.LIFT + m * NP + i), s_f[w][m], lift);
+      A.visc[(int64_t)r * NP + i] = div + lift;
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -331,12 +324,6 @@ size_t ls_sensor_smem() {
 }
 
 template <int N>
-size_t ls_sparse_smem() {
-  constexpr int NP = Order<N>::NP, NF = Order<N>::NF;
-  return sizeof(double) * (3 * NP * NP + NP * NF + 3 * NP + 3 * NF);
-}
-
-template <int N>
 void ls_attrs() {
   static bool done[64] = {};
   int dev = 0;
@@ -345,18 +332,11 @@ void ls_attrs() {
   cuda_check(cudaFuncSetAttribute(ls_sensor_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)ls_sensor_smem<N>()),
              "ls_sensor smem");
-  cuda_check(cudaFuncSetAttribute(ls_grad_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)ls_sparse_smem<N>()),
-             "ls_grad smem");
-  cuda_check(cudaFuncSetAttribute(ls_div_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)ls_sparse_smem<N>()),
-             "ls_div smem");
   if (dev >= 0 && dev < 64) done[dev] = true;
 }
 
 template <int N>
 void launch_ls_n(const LsArgs &A, int num_sms, cudaStream_t st) {
-  static_assert(Order<N>::NP <= kLsThreads && Order<N>::NF <= kLsThreads, "one thread per node and face point");
   ls_attrs<N>();
   cuda_check(cudaMemsetAsync(A.counts, 0, 3 * sizeof(int32_t), st), "reset counts");
   const int gs = std::max(1, std::min(2 * A.ntiles, num_sms * 8));
@@ -366,9 +346,9 @@ void launch_ls_n(const LsArgs &A, int num_sms, cudaStream_t st) {
   cuda_check(cudaGetLastError(), "ls_touch_kernel launch");
   ls_compact_kernel<<<num_sms * 4, 256, 0, st>>>(A);
   cuda_check(cudaGetLastError(), "ls_compact_kernel launch");
-  ls_grad_kernel<N><<<num_sms * 4, kLsThreads, ls_sparse_smem<N>(), st>>>(A);
+  ls_grad_kernel<N><<<num_sms * 8, 32 * kLsWarps, 0, st>>>(A);
   cuda_check(cudaGetLastError(), "ls_grad_kernel launch");
-  ls_div_kernel<N><<<num_sms * 4, kLsThreads, ls_sparse_smem<N>(), st>>>(A);
+  ls_div_kernel<N><<<num_sms * 8, 32 * kLsWarps, 0, st>>>(A);
   cuda_check(cudaGetLastError(), "ls_div_kernel launch");
 }
 

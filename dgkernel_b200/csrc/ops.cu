@@ -593,11 +593,18 @@ struct MixedOp : Op {
       Binding *Vi = R.matrix("Vinv");
       require(Vi->rows == np && Vi->cols == np, R.kname + ": Vinv must be Np x Np");
       auto rm = [&](const std::vector<double> &m, DevBuf &d) { d.upload(m.data(), m.size() * sizeof(double)); };
-      rm(Dr->mat, l_dr);
-      rm(Ds->mat, l_ds);
-      rm(Dt->mat, l_dt);
+      // the sparse passes read Dr, Ds, Dt and LIFT transposed (column j contiguous over rows i)
+      auto tr = [&](const std::vector<double> &m, int64_t rows, int64_t cols, DevBuf &d) {
+        std::vector<double> t((size_t)(rows * cols));
+        for (int64_t i = 0; i < rows; ++i)
+          for (int64_t j = 0; j < cols; ++j) t[(size_t)(j * rows + i)] = m[(size_t)(i * cols + j)];
+        d.upload(t.data(), t.size() * sizeof(double));
+      };
+      tr(Dr->mat, np, np, l_dr);
+      tr(Ds->mat, np, np, l_ds);
+      tr(Dt->mat, np, np, l_dt);
       rm(Vi->mat, l_vinv);
-      rm(L->mat, l_lift);
+      tr(L->mat, np, nf, l_lift);
       if (lmode >= 2) {
         mlpB = R.matrix("MLP");
         require(mlpB->rows * mlpB->cols == mlp_param_count((int)np) && mlpB->dev_dtype == DGK_FLOAT32,
