@@ -51,6 +51,8 @@ SIGNATURES = {
     "dgk_halo_plan": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI32, _I32, _I32, _PI64, _PI64, _PI32, _PI64,
                       _PI64, _PI64, _PI64],
     "dgk_gather_values": [_P, _I32, _I64, _P, _I64, _P, _P],
+    "dgk_tile_halo": [_I32, _PI64, _PI64, _I32, _I32, _PI32, _I32, _I32, _I32, _I32, _I32, _PI64, _PI32, _PI64,
+                      _PI32, _PI32, _PI32, C.POINTER(C.c_uint32)],
     "dgk_face_gather_map": [_I64, _I32, _I32, _I32, _PI64, _PI64, _I32, _PI64, _PI32],
     "dgk_init_field_parts": [_P, _S, _S, _S, _S, _D, _I32, _PD],
     "dgk_mlp_param_count": [_I32, _PI64],

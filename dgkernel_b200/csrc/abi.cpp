@@ -298,6 +298,33 @@ int dgk_compact_faces(int32_t npart, const int64_t *K, const int64_t *node_off, 
   });
 }
 
+int dgk_tile_halo(int32_t npart, const int64_t *K, const int64_t *node_off, int32_t Np, int32_t Nfp,
+                  const int32_t *conn, int32_t max_elems, int32_t max_halo, int32_t halo_floats, int32_t identity_code,
+                  int32_t align, int64_t *counts_out, int32_t *part_out, int64_t *first_out, int32_t *nelem_out,
+                  int32_t *halo_off_out, int32_t *halo_list_out, uint32_t *tconn_out) {
+  return guard(nullptr, [&] {
+    if (npart < 1 || !K || !node_off || !conn || !counts_out)
+      throw dgk::Error(DGK_ERR_INVALID, "tile halo: null argument or npart < 1");
+    std::vector<int64_t> sp((size_t)npart + 1, 0);
+    for (int p = 0; p < npart; ++p) sp[(size_t)p + 1] = sp[(size_t)p] + dgk::slot_padded(K[p]);
+    dgk::TileHalo th;
+    try {
+      th = dgk::tile_halo(npart, K, node_off, sp.data(), Np, Nfp, conn, max_elems, max_halo, halo_floats,
+                          identity_code, align);
+    } catch (const std::runtime_error &ex) {
+      throw dgk::Error(DGK_ERR_INVALID, ex.what());
+    }
+    counts_out[0] = (int64_t)th.nelem.size();
+    counts_out[1] = (int64_t)th.halo_list.size() / 2;
+    if (part_out) std::copy(th.part.begin(), th.part.end(), part_out);
+    if (first_out) std::copy(th.first.begin(), th.first.end(), first_out);
+    if (nelem_out) std::copy(th.nelem.begin(), th.nelem.end(), nelem_out);
+    if (halo_off_out) std::copy(th.halo_off.begin(), th.halo_off.end(), halo_off_out);
+    if (halo_list_out) std::copy(th.halo_list.begin(), th.halo_list.end(), halo_list_out);
+    if (tconn_out) std::copy(th.tconn.begin(), th.tconn.end(), tconn_out);
+  });
+}
+
 int dgk_splitmix_uniform(uint64_t seed, int64_t count, double *out) {
   uint64_t s = seed;
   for (int64_t i = 0; i < count; ++i) out[i] = dgk::splitmix_uniform(s);

@@ -109,11 +109,13 @@ struct MixedArgs {
   float *uhi_out, *ulo_out;      // state written by this stage (ping-pong partners)
   float *resu;                   // LSERK residual, updated in place
   const float *geo;              // kMixedGeoWords per element slot
-  const int32_t *conn;           // kMixedConnWords per element slot
+  const int32_t *conn;           // kMixedConnWords per element slot (tensor-core form: 4 tile-local words)
   int64_t n_u_values;            // bound of every gathered value index
   const float *Dm;               // [NP][NPJ][3]: Dr, Ds, Dt entries interleaved per column, zero-padded
   const float *lift;             // [NP][4 Nfp]
   const unsigned char *bmat;     // tensor-core form: split BF16 operands of D and LIFT (tcm_pack_operands)
+  const int32_t *halo_off;       // tensor-core form: per tile, first entry of its halo list (ntiles + 1)
+  const int32_t *halo_list;      // tensor-core form: (neighbour base, face-order code) per halo face
   const int32_t *vslot;          // tensor-core form with viscosity: per element slot, row of visc or -1
   const double *visc;            // [row][Np] viscous right-hand side added before the update
   const double *bary;            // [NP][3] barycentric weights of vertices B, C, D at each node

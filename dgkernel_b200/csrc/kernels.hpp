@@ -35,10 +35,13 @@ bool launch_rhs_mixed(int N, const MixedArgs &A, int consumer_warps, int ring_ma
                       LaunchInfo *info);
 void prepare_rhs_mixed(int N, int consumer_warps);  // attributes, before any stream capture
 uint32_t mixed_slot_bytes(int N);  // 0 when the order has no such form
-// Mixed stage with the element-local products on the tensor cores (tcm.cu), orders 1..4: tiles of
-// tcm_tile_elems() elements; the operand buffer comes from tcm_pack_operands (Dr, Ds, Dt, LIFT row-major FP64).
+// Mixed stage with the element-local products on the tensor cores (tcm.cu), orders 1..4: tiles of at most
+// tcm_tile_elems() elements and tcm_halo_capacity() halo faces (tile_halo, with halo positions from
+// tcm_halo_floats(N)); the operand buffer comes from tcm_pack_operands (Dr, Ds, Dt, LIFT row-major FP64).
 bool tcm_supported(int N);
 int tcm_tile_elems();
+int tcm_halo_capacity();
+int tcm_halo_floats(int N);
 void tcm_pack_operands(int N, const double *Dr, const double *Ds, const double *Dt, const double *LIFT,
                        std::vector<uint16_t> &out);
 // consumer_warps 8 or 16 (2 or 4 threads per element)

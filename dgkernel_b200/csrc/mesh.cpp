@@ -263,6 +263,84 @@ CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off,
   return out;
 }
 
+TileHalo tile_halo(int npart, const int64_t *K, const int64_t *node_off, const int64_t *slot_prefix, int Np, int Nfp,
+                   const int32_t *conn, int max_elems, int max_halo, int halo_floats, int identity_code, int align) {
+  if (align < 1 || max_elems < align || max_halo < 4 * align || (max_halo & 1))
+    throw std::runtime_error("tile halo: limits must satisfy max_elems >= align, max_halo >= 4 align, max_halo even");
+  if ((int64_t)max_elems * Np > halo_floats || (int64_t)halo_floats + (int64_t)max_halo * Nfp > 65536)
+    throw std::runtime_error("tile halo: slot positions do not fit 16 bits");
+  if (identity_code < 0 || identity_code > 255) throw std::runtime_error("tile halo: identity code outside 8 bits");
+  TileHalo out;
+  out.tconn.assign((size_t)(slot_prefix[npart] * 4), 0u);
+  out.halo_off.push_back(0);
+  for (int p = 0; p < npart; ++p) {
+    const int64_t lo = node_off[p], hi = node_off[p] + K[p] * Np;
+    // partition-local element of the face-f neighbour of element e; -1 outside this partition
+    auto nbr = [&](int64_t e, int f) -> int64_t {
+      const int64_t nb = conn[(size_t)((slot_prefix[p] + e) * 5 + f)];
+      return (nb >= lo && nb < hi) ? (nb - lo) / Np : -1;
+    };
+    for (int64_t s0 = 0; s0 < K[p];) {
+      // grow the tile one element at a time, keeping the count of faces whose neighbour lies outside it; the
+      // tile is the longest prefix that ends on an aligned boundary (or the partition's end) within max_halo
+      const int64_t mmax = std::min<int64_t>(max_elems, K[p] - s0);
+      int64_t best = 0;
+      int64_t c = 0;
+      for (int64_t m = 1; m <= mmax; ++m) {
+        const int64_t x = s0 + m - 1;
+        int64_t seen[4];
+        int ns = 0;
+        for (int f = 0; f < 4; ++f) {
+          const int64_t y = nbr(x, f);
+          if (y < s0 || y > x) {
+            ++c;  // neighbour outside the tile so far
+            continue;
+          }
+          if (y == x) continue;  // a face whose neighbour is the element itself
+          bool dup = false;
+          for (int i = 0; i < ns; ++i) dup |= seen[i] == y;
+          if (dup) continue;
+          seen[ns++] = y;
+          for (int g = 0; g < 4; ++g) c -= nbr(y, g) == x;  // y's faces towards x are inside now
+        }
+        if (c <= max_halo && (m % align == 0 || s0 + m == K[p])) best = m;
+      }
+      if (best == 0) throw std::runtime_error("tile halo: an aligned group of elements exceeds the halo capacity");
+      int32_t j = 0;
+      for (int64_t e = s0; e < s0 + best; ++e) {
+        const int64_t sl = slot_prefix[p] + e;
+        const uint32_t codes = (uint32_t)conn[(size_t)(sl * 5 + 4)];
+        for (int f = 0; f < 4; ++f) {
+          const int64_t y = nbr(e, f);
+          const uint32_t code = (codes >> (8 * f)) & 0xffu;
+          uint32_t word;
+          if (y >= s0 && y < s0 + best) {
+            word = (uint32_t)((y - s0) * Np) | (code << 16);
+          } else {
+            out.halo_list.push_back(conn[(size_t)(sl * 5 + f)]);
+            out.halo_list.push_back((int32_t)code);
+            word = (uint32_t)(halo_floats + j * Nfp) | ((uint32_t)identity_code << 16);
+            ++j;
+          }
+          out.tconn[(size_t)(sl * 4 + f)] = word;
+        }
+      }
+      if (j & 1) {  // even entry count (16-byte copies): repeat the last entry
+        const size_t n = out.halo_list.size();
+        out.halo_list.push_back(out.halo_list[n - 2]);
+        out.halo_list.push_back(out.halo_list[n - 1]);
+      }
+      if (out.halo_list.size() / 2 > (size_t)INT32_MAX) throw std::runtime_error("tile halo: more than 2^31 entries");
+      out.halo_off.push_back((int32_t)(out.halo_list.size() / 2));
+      out.part.push_back(p);
+      out.first.push_back(s0);
+      out.nelem.push_back((int32_t)best);
+      s0 += best;
+    }
+  }
+  return out;
+}
+
 uint64_t splitmix_next(uint64_t &state) {
   state += 0x9E3779B97F4A7C15ull;
   uint64_t z = state;

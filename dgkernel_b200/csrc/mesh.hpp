@@ -34,6 +34,24 @@ CompactFaces compact_faces(int npart, const int64_t *K, const int64_t *node_off,
                            const int64_t *slot_prefix, int Np, int Nfp, const int32_t *gmap);
 int64_t slot_padded(int64_t k);  // k rounded up to whole 32-element slots
 
+// Tiles of the tensor-core mixed stage with their halos.  Each partition is cut into runs of consecutive
+// elements (tiles) of at most max_elems elements, whose first element is a multiple of `align`, and whose
+// faces with a neighbour outside the tile number at most max_halo.  Per tile: the halo list (neighbour base,
+// face-order code) of those faces, padded to an even entry count; per element slot (slot_prefix layout):
+// four words, word f = the face-f neighbour trace's position in the tile's shared-memory slot
+// (low 16 bits, in floats from the slot's first value: (neighbour - first element) * Np inside the tile,
+// halo_floats + j * Nfp for halo face j) | code << 16, where halo faces carry identity_code (their values
+// are stored in this face's point order).  conn is compact_faces' layout.
+struct TileHalo {
+  std::vector<int32_t> part, nelem;
+  std::vector<int64_t> first;      // partition-local first element of each tile
+  std::vector<int32_t> halo_off;   // ntiles + 1 entry offsets into halo_list (pairs)
+  std::vector<int32_t> halo_list;  // (neighbour base, code) per halo face
+  std::vector<uint32_t> tconn;     // 4 words per element slot
+};
+TileHalo tile_halo(int npart, const int64_t *K, const int64_t *node_off, const int64_t *slot_prefix, int Np, int Nfp,
+                   const int32_t *conn, int max_elems, int max_halo, int halo_floats, int identity_code, int align);
+
 // Exchange plan of one rank when partitions are spread over ranks (part_rank[p]), built from the FaceConnector
 // pick/place lists (utils/face_connector.go:143-187).  The rank's state array holds its partitions at
 // local_off[0..L-1] (value offsets, ascending partition id) and a halo at local_off[L].  For peer rank q the

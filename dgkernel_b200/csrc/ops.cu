@@ -392,6 +392,7 @@ struct MixedOp : Op {
   int N = 0, ntiles = 0, conservative = 0, ncodes = 0, warps = 11, ring = 0, tensor = 0, mma = 0;
   Binding *uhi, *ulo, *uhin, *ulon, *resu;
   DevBuf tiles, geoE, conn, dm, lift, bary, vtx, ftab, fmask, amat, rexp, bmat;
+  DevBuf tconn, hoff, hlist;  // tensor-core form: tile-local connectivity and the tiles' halo lists
   // learned-sensor viscosity (sensor=pp|mlp|mlp0 with mma=1)
   int lmode = 0;
   double eps0 = 1.0, s0 = 0.0, kappa = 1.0;
@@ -513,9 +514,26 @@ struct MixedOp : Op {
     } catch (const std::exception &ex) {
       throw Error(DGK_ERR_INVALID, R.kname + ": " + ex.what());
     }
-    ncodes = std::max(cf.ncodes, 1);
-    if (cf.table.empty()) cf.table.assign((size_t)nfp, 0);
     conn.upload(cf.conn.data(), std::max<size_t>(cf.conn.size(), 1) * sizeof(int32_t));
+    TileHalo th;
+    if (mma) {
+      // tiles with their halos; a halo face's values arrive in the face's own point order: the identity row
+      try {
+        th = tile_halo(P, r.K.data(), uhi->offsets.data(), slot_prefix.data(), (int)np, nfp, cf.conn.data(),
+                       tcm_tile_elems(), tcm_halo_capacity(), tcm_halo_floats(N), cf.ncodes, 4);
+      } catch (const std::exception &ex) {
+        throw Error(DGK_ERR_INVALID, R.kname + ": " + ex.what());
+      }
+      for (int i = 0; i < nfp; ++i) cf.table.push_back((uint8_t)i);
+      ncodes = cf.ncodes + 1;
+      tconn.upload(th.tconn.data(), std::max<size_t>(th.tconn.size(), 1) * sizeof(uint32_t));
+      hoff.upload(th.halo_off.data(), th.halo_off.size() * sizeof(int32_t));
+      th.halo_list.resize(std::max<size_t>(th.halo_list.size(), 4), 0);
+      hlist.upload(th.halo_list.data(), th.halo_list.size() * sizeof(int32_t));
+    } else {
+      ncodes = std::max(cf.ncodes, 1);
+      if (cf.table.empty()) cf.table.assign((size_t)nfp, 0);
+    }
     ftab.upload(cf.table.data(), cf.table.size());
     // Dr, Ds, Dt interleaved by column pairs ([i][j/2][r,s,t][j%2]), columns padded to a multiple of 4 with
     // zeros: one row's pair of columns feeds three paired FMAs
@@ -557,18 +575,23 @@ struct MixedOp : Op {
       tcm_pack_operands(N, Dr->mat.data(), Ds->mat.data(), Dt->mat.data(), L->mat.data(), packed);
       bmat.upload(packed.data(), packed.size() * sizeof(uint16_t));
     }
-    const int te = tensor ? oz_tile_elems() : mma ? tcm_tile_elems() : kMixedSlotElems;
+    const int te = tensor ? oz_tile_elems() : kMixedSlotElems;
     std::vector<MTile> tl;
-    for (int p = 0; p < P; ++p)
-      for (int64_t s0 = 0; s0 < r.K[p]; s0 += te) {
-        MTile x;
-        x.node_base = uhi->offsets[p] + s0 * np;
-        x.elem_slot = slot_prefix[p] + s0;
-        x.nelem = (int32_t)std::min<int64_t>(te, r.K[p] - s0);
-        x.part = p;
-        require((x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
-        tl.push_back(x);
-      }
+    auto add_tile = [&](int p, int64_t s0, int64_t ne) {
+      MTile x;
+      x.node_base = uhi->offsets[p] + s0 * np;
+      x.elem_slot = slot_prefix[p] + s0;
+      x.nelem = (int32_t)ne;
+      x.part = p;
+      require((x.node_base * 4) % 16 == 0, R.kname + ": partition offsets of uhi must be 16-byte aligned");
+      tl.push_back(x);
+    };
+    if (mma) {
+      for (size_t i = 0; i < th.nelem.size(); ++i) add_tile(th.part[i], th.first[i], th.nelem[i]);
+    } else {
+      for (int p = 0; p < P; ++p)
+        for (int64_t s0 = 0; s0 < r.K[p]; s0 += te) add_tile(p, s0, std::min<int64_t>(te, r.K[p] - s0));
+    }
     ntiles = (int)tl.size();
     tiles.upload(tl.data(), std::max<size_t>(tl.size(), 1) * sizeof(MTile));
     const std::string sensor = lower(R.word("sensor", "none"));
@@ -765,6 +788,9 @@ struct MixedOp : Op {
     A.status = r.status_word();
     if (mma) {
       A.bmat = bmat.get<unsigned char>();
+      A.conn = tconn.get<int32_t>();
+      A.halo_off = hoff.get<int32_t>();
+      A.halo_list = hlist.get<int32_t>();
       if (lmode) {
         launch_viscosity(r);
         A.vslot = l_vslot.get<int32_t>();

@@ -3,29 +3,32 @@
 // Same arithmetic contract as rhs_stage_mixed_kernel (mixed.cu): the state is a compensated FP32 pair
 // (u = hi + lo), the residual FP32; the derivative operand is w minus its linear vertex
 // interpolant (w = u or u^2/2), whose exact derivative is added back; the Lax-Friedrichs flux is formed in
-// FP32.  The two products per element, D{r,s,t} dw and LIFT flux, run as GEMMs over tiles of 128 elements:
+// FP32.  The two products per element, D{r,s,t} dw and LIFT flux, run as GEMMs over tiles of up to 128
+// elements:
 //
 //   acc_V[e][3i+d] = sum_j dw[e][j] D_d[i][j]      M = 128 elements, N = rup16(3 Np), K = rup16(Np)
 //   acc_L[e][i]    = sum_m fl[e][m] LIFT[i][m]     M = 128 elements, N = rup16(Np),   K = 4 rup8(Nfp)
 //                                                  (face-major K, each face's points padded to 8)
 //
-// with elements on the MMA's M dimension, so that TMEM lane e holds element e's outputs and the threads that
-// own element e read them back.  Every operand is split into three BF16 parts, x = x0 + x1 + x2 (x0 = bf16(x),
-// x1 = bf16(x - x0), x2 = bf16(x - x0 - x1), about 24 significant bits), and a product keeps the six terms
-// a_p b_q with p + q <= 2, all accumulated in one FP32 TMEM accumulator: the products carry FP32-level
-// rounding (the dropped terms are below 2^-24 of the product).
+// with elements on the MMA's M dimension, so that TMEM lane e holds element e's operand rows and outputs and
+// the threads that own element e write and read them.  Every operand is split into three BF16 parts,
+// x = x0 + x1 + x2 (x0 = bf16(x), x1 = bf16(x - x0), x2 = bf16(x - x0 - x1), about 24 significant bits), and
+// a product keeps the six terms a_p b_q with p + q <= 2, all accumulated in one FP32 TMEM accumulator: the
+// products carry FP32-level rounding (the dropped terms are below 2^-24 of the product).
 //
-// CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry and connectivity into a
-// 2-slot ring with 1-D bulk copies and writes finished slots back with bulk stores; one MMA warp issues the
-// GEMMs; CW consumer warps hold CW / 4 threads per element (warps w, w + 4, ... share the TMEM lane quarter
-// w mod 4 and split the element's nodes in 8-wide chunks and its faces).  Per tile: the consumer threads write
-// the split dw into the A buffer (K-major canonical layout) and arrive on an mbarrier, on which the MMA warp
-// issues the volume MMAs; they form the flux meanwhile, write it into the same A buffer once the volume MMAs
-// have completed and arrive again for the LIFT MMAs; then they read both accumulators from TMEM and finish the
-// stage (the compensated update in error-free FP32 arithmetic) into the slot.  No barrier among the consumers
-// within a tile.  Constant operands (D and LIFT, split) stay in shared memory for the whole launch.  Every wait
-// is bounded; a failed wait sets the status word and the CTA leaves after draining its copies and MMAs; TMEM is
-// always freed.
+// CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry and tile-local
+// connectivity into a 2-slot ring with 1-D bulk copies, gathers the tile's halo (the traces of neighbours
+// outside the tile, listed per tile by the host) into the slot with 4-byte asynchronous copies, and writes
+// finished slots back with bulk stores; one MMA warp issues the GEMMs with operand A read from tensor memory
+// and operand B (D and LIFT, split) from shared memory, where it stays for the whole launch; CW consumer warps
+// hold CW / 4 threads per element (warps w, w + 4, ... share the TMEM lane quarter w mod 4 and split the
+// element's nodes in 8-wide chunks and its faces).  Per tile: the consumer threads read their faces'
+// neighbour traces from the slot (inside the tile, or the halo), store the split dw into TMEM and arrive on
+// an mbarrier, on which the MMA warp issues the volume GEMM; they form the flux meanwhile, store it into its
+// own TMEM columns and arrive again for the LIFT GEMM; then they read both accumulators and finish the stage
+// (the compensated update in error-free FP32 arithmetic) into the slot.  No barrier among the consumers within
+// a tile.  Every wait is bounded; a failed wait sets the status word and the CTA leaves after draining its
+// copies and MMAs; TMEM is always freed.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -41,8 +44,9 @@ namespace dgk {
 
 namespace {
 
-constexpr int kTmTE = 128;    // elements per tile (the MMA's M)
-constexpr int kTmCols = 256;  // TMEM columns (volume and LIFT accumulators)
+constexpr int kTmTE = 128;    // elements per tile at most (the MMA's M)
+constexpr int kTmHalo = 256;  // halo faces per tile at most (even)
+constexpr int kTmCols = 512;  // TMEM columns: accumulators, then the split A operands
 
 template <int N>
 struct TmCfg {
@@ -51,23 +55,32 @@ struct TmCfg {
   // LIFT's K runs face-major, each face padded to KF columns: column f KF + p holds face f's point p
   static constexpr int KF = (NFP + 7) & ~7;
   static constexpr int KV = rup16(NP), KL = rup16(4 * KF), NV = rup16(3 * NP), NL = rup16(NP);
-  static constexpr int KA = KV > KL ? KV : KL;
   static constexpr uint32_t BV_PART = (uint32_t)NV * KV * 2, BL_PART = (uint32_t)NL * KL * 2;
-  static constexpr uint32_t A_PART = (uint32_t)kTmTE * KA * 2;
+  // slot layout (bytes from the slot's start): hi, lo, resu, geometry, tile-local connectivity, halo list,
+  // halo values (NFP floats per halo face, in the face's point order)
   static constexpr uint32_t NODE_B = (uint32_t)kTmTE * NP * 4;
   static constexpr uint32_t GEO_B = (uint32_t)kTmTE * kMixedGeoWords * 4;
-  static constexpr uint32_t CONN_B = (uint32_t)kTmTE * kMixedConnWords * 4;
-  static constexpr uint32_t SLOT_B = 3 * NODE_B + GEO_B + CONN_B;
+  static constexpr uint32_t TC_B = (uint32_t)kTmTE * 4 * 4;
+  static constexpr uint32_t HL_B = (uint32_t)kTmHalo * 8;
+  static constexpr uint32_t HV_B = round16((uint32_t)kTmHalo * NFP * 4);
+  static constexpr uint32_t S_GEO = 3 * NODE_B, S_TC = S_GEO + GEO_B, S_HL = S_TC + TC_B, S_HV = S_HL + HL_B;
+  static constexpr uint32_t SLOT_B = S_HV + HV_B;
+  static constexpr int HALO_FLOATS = (int)(S_HV / 4), SLOT_FLOATS = (int)(SLOT_B / 4);
   // shared-memory layout (bytes)
-  static constexpr uint32_t OFF_BV = 0, OFF_BL = OFF_BV + 3 * BV_PART, OFF_A = OFF_BL + 3 * BL_PART;
-  static constexpr uint32_t OFF_SLOT = OFF_A + 3 * A_PART, OFF_BARY = OFF_SLOT + 2 * SLOT_B;
-  // full[2], done[2], mvol, mlift, avol, alift
+  static constexpr uint32_t OFF_BV = 0, OFF_BL = OFF_BV + 3 * BV_PART, OFF_SLOT = OFF_BL + 3 * BL_PART;
+  static constexpr uint32_t OFF_BARY = OFF_SLOT + 2 * SLOT_B;
+  // full[2], done[2], mvol, mlift, avol, alift, lst[2], hfree[2]
   static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;
-  static constexpr uint32_t OFF_MISC = OFF_BARS + 8 * 8;  // abort flag, TMEM base
+  static constexpr uint32_t OFF_MISC = OFF_BARS + 12 * 8;  // abort flag, TMEM base
   static constexpr uint32_t OFF_FMASK = (OFF_MISC + 16 + 15) & ~15u;
   static constexpr uint32_t OFF_FTAB = OFF_FMASK + ((NF + 15) & ~15);  // face-order rows of 16 bytes
   static constexpr uint32_t CONST_BYTES = 3 * BV_PART + 3 * BL_PART;  // the packed operand buffer
-  static_assert(3 * NP <= 256 && NP <= 128 && NFP <= 16, "tile shapes");
+  // TMEM columns: acc_V, acc_L, then the three parts of the volume operand and of the LIFT operand (32
+  // columns, 64 BF16 values of K, per part)
+  static constexpr uint32_t T_ACCV = 0, T_ACCL = NV, T_AV = (uint32_t)((NV + NL + 31) & ~31), T_AL = T_AV + 3 * 32;
+  static_assert(3 * NP <= 256 && NP <= 128 && NFP <= 16 && KV <= 64 && KL <= 64, "tile shapes");
+  static_assert(T_AL + 3 * 32 <= (uint32_t)kTmCols, "TMEM columns");
+  static_assert(HALO_FLOATS + kTmHalo * NFP <= 65536 && kTmTE * NP <= HALO_FLOATS, "16-bit slot positions");
 };
 
 template <int N>
@@ -84,8 +97,9 @@ __device__ __forceinline__ uint32_t bf16_pair(float &x, float &y) {
   return w;
 }
 
-// Split 8 values into three BF16 parts and store each part's 16 bytes at `dst + p * part_bytes`.
-__device__ __forceinline__ void store_split8(unsigned char *dst, uint32_t part_bytes, const float (&v)[8]) {
+// Split 8 consecutive K values of this thread's row into three BF16 parts and store part p's four packed
+// columns at TMEM column `col + 32 p` of this warp's lanes.
+__device__ __forceinline__ void tmem_split8(uint32_t col, const float (&v)[8]) {
   uint32_t w0[4], w1[4], w2[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
@@ -94,9 +108,9 @@ __device__ __forceinline__ void store_split8(unsigned char *dst, uint32_t part_b
     w1[q] = bf16_pair(x, y);
     w2[q] = bf16_pair(x, y);
   }
-  *reinterpret_cast<uint4 *>(dst) = make_uint4(w0[0], w0[1], w0[2], w0[3]);
-  *reinterpret_cast<uint4 *>(dst + part_bytes) = make_uint4(w1[0], w1[1], w1[2], w1[3]);
-  *reinterpret_cast<uint4 *>(dst + 2 * part_bytes) = make_uint4(w2[0], w2[1], w2[2], w2[3]);
+  tmem_st4(col, w0[0], w0[1], w0[2], w0[3]);
+  tmem_st4(col + 32, w1[0], w1[1], w1[2], w1[3]);
+  tmem_st4(col + 64, w2[0], w2[1], w2[2], w2[3]);
 }
 
 // 24 consecutive TMEM columns (three 8-column loads) of this warp's lanes under one wait.
@@ -130,17 +144,17 @@ __device__ __forceinline__ void stage_update(float hi, float lo, float rn, float
   ln = (s - (hn - bt)) + (t - bt);  // s + t = hn + ln exactly
 }
 
-// One GEMM of the split products: 6 MMAs per 16-wide K step into the accumulator at `acc`.
-__device__ __forceinline__ void split_gemm(uint32_t acc, uint32_t a0, uint32_t a_part, uint32_t b0, uint32_t b_part,
-                                           int K, int NB, uint32_t idesc) {
+// One GEMM of the split products: 6 MMAs per 16-wide K step into the accumulator at `acc`; A's three parts at
+// TMEM columns a0, a0 + 32, a0 + 64 (8 columns per K step), B's in shared memory.
+__device__ __forceinline__ void split_gemm(uint32_t acc, uint32_t a0, uint32_t b0, uint32_t b_part, int K, int NB,
+                                           uint32_t idesc) {
   const int pa[6] = {0, 0, 1, 0, 2, 1}, pb[6] = {0, 1, 0, 2, 0, 1};
   for (int ks = 0; ks < K / 16; ++ks) {
-    const uint32_t ao = (uint32_t)ks * 2 * (kTmTE / 8) * 128, bo = (uint32_t)ks * 2 * (NB / 8) * 128;
+    const uint32_t bo = (uint32_t)ks * 2 * (NB / 8) * 128;
 #pragma unroll
     for (int t = 0; t < 6; ++t) {
-      const uint64_t da = smem_desc(a0 + pa[t] * a_part + ao, (kTmTE / 8) * 128, 128);
       const uint64_t db = smem_desc(b0 + pb[t] * b_part + bo, (NB / 8) * 128, 128);
-      tc_mma(acc, da, db, idesc, (ks > 0 || t > 0) ? 1u : 0u);
+      tc_mma_ts(acc, a0 + 32u * pa[t] + 8u * ks, db, idesc, (ks > 0 || t > 0) ? 1u : 0u);
     }
   }
 }
@@ -162,17 +176,20 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
   constexpr int NP = C::NP, NFP = C::NFP, NF = C::NF, KV = C::KV, KL = C::KL, NV = C::NV, NL = C::NL;
   constexpr int TE = kTmTE;
   extern __shared__ __align__(1024) unsigned char sm[];
-  unsigned char *sBV = sm + C::OFF_BV, *sBL = sm + C::OFF_BL, *sA = sm + C::OFF_A;
+  unsigned char *sBV = sm + C::OFF_BV, *sBL = sm + C::OFF_BL;
   unsigned char *ring = sm + C::OFF_SLOT;
   double *sBary = reinterpret_cast<double *>(sm + C::OFF_BARY);
-  // full: slot filled (producer's copies); done: slot finished (every consumer thread); mvol / mlift: MMA group
-  // complete (tcgen05.commit); avol / alift: operand written into the A buffer (every consumer thread)
+  // full: slot filled (the producer's bulk copies, and every producer lane's halo copies); done: slot finished
+  // (every consumer thread); mvol / mlift: MMA group complete (tcgen05.commit); avol / alift: operand written
+  // into TMEM (every consumer thread); lst: a slot's halo list arrived; hfree: every consumer thread has read
+  // the slot's halo
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *done = full + 2, *mvol = full + 4,
-           *mlift = full + 5, *avol = full + 6, *alift = full + 7;
+           *mlift = full + 5, *avol = full + 6, *alift = full + 7, *lst = full + 8, *hfree = full + 10;
   int *sMisc = reinterpret_cast<int *>(sm + C::OFF_MISC);  // [0] abort flag, [1] TMEM base
   uint8_t *sFm = sm + C::OFF_FMASK, *sFt = sm + C::OFF_FTAB;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int G = gridDim.x;
+  const int ncodes = A.ncodes;
 
   // constant operands, tables and barriers
   {
@@ -182,9 +199,18 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
   }
   for (int x = tid; x < NP * 3; x += blockDim.x) sBary[x] = A.bary[x];
   for (int x = tid; x < NF; x += blockDim.x) sFm[x] = (uint8_t)A.fmask[x];
-  for (int x = tid; x < A.ncodes * 16; x += blockDim.x) sFt[x] = (x & 15) < NFP ? A.ftab[(x >> 4) * NFP + (x & 15)] : 0;
+  for (int x = tid; x < ncodes * 16; x += blockDim.x) sFt[x] = (x & 15) < NFP ? A.ftab[(x >> 4) * NFP + (x & 15)] : 0;
   if (tid == 0) {
-    for (int b = 0; b < 8; ++b) mbar_init(&full[b], (b == 2 || b == 3 || b >= 6) ? 32 * CW : 1);
+    for (int b = 0; b < 2; ++b) mbar_init(&full[b], 1 + 32);  // the bulk copies' arrival and 32 producer lanes
+    for (int b = 2; b < 4; ++b) mbar_init(&full[b], 32 * CW);
+    mbar_init(mvol, 1);
+    mbar_init(mlift, 1);
+    mbar_init(avol, 32 * CW);
+    mbar_init(alift, 32 * CW);
+    mbar_init(&lst[0], 1);
+    mbar_init(&lst[1], 1);
+    mbar_init(&hfree[0], 32 * CW);
+    mbar_init(&hfree[1], 32 * CW);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     sMisc[0] = 0;
   }
@@ -200,71 +226,129 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
   const uint32_t tmem = (uint32_t)sMisc[1];
 
   if (warp == CW + 1) {
-    // producer, lane 0: streams this CTA's tiles through the 2-slot ring and writes each finished slot back.
-    // Slot s holds tile k, then k + 2: once every consumer thread has arrived on done[s] for tile k, the slot's
-    // hi, lo and resu go out with bulk stores (the ragged tail past the last full 16 bytes was written by the
-    // consumers), and the refill starts when the stores have read the slot.
-    if (lane == 0) {
-      MTile held[2] = {};
-      auto store = [&](int s, const MTile &tl) {
-        const uint32_t nbd = (((uint32_t)(tl.nelem * NP * 4)) & ~15u);
-        unsigned char *slot = ring + (size_t)s * C::SLOT_B;
-        if (nbd) {
-          bulk_s2g(A.uhi_out + tl.node_base, slot, nbd);
-          bulk_s2g(A.ulo_out + tl.node_base, slot + C::NODE_B, nbd);
-          bulk_s2g(A.resu + tl.node_base, slot + 2 * C::NODE_B, nbd);
+    // producer warp.  Slot s holds tile k, then k + 2.  Per tile: lane 0 requests the tile's halo list (only
+    // this warp reads the list region, and it has finished with tile k - 2's); once every consumer thread has
+    // read tile k - 2's halo (hfree[s]) and the list has landed, every lane gathers its share of the halo values
+    // with 4-byte asynchronous copies and arrives on full[s] when they have landed.  Then lane 0 waits until
+    // every consumer thread has finished tile k - 2 (done[s]), writes its hi, lo and resu out with bulk stores
+    // (the ragged tail past the last full 16 bytes was written by the consumers) and refills the slot once the
+    // stores have read it.
+    MTile held[2] = {};
+    int kl[2] = {-1, -1}, kf[2] = {-1, -1};  // newest list request and newest fill of each slot (lane 0)
+    const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
+    auto store = [&](int s, const MTile &tl) {
+      const uint32_t nbd = (((uint32_t)(tl.nelem * NP * 4)) & ~15u);
+      unsigned char *slot = ring + (size_t)s * C::SLOT_B;
+      if (nbd) {
+        bulk_s2g(A.uhi_out + tl.node_base, slot, nbd);
+        bulk_s2g(A.ulo_out + tl.node_base, slot + C::NODE_B, nbd);
+        bulk_s2g(A.resu + tl.node_base, slot + 2 * C::NODE_B, nbd);
+      }
+      bulk_commit();
+    };
+    int k = 0;
+    bool bad = false;
+    for (;; ++k) {
+      const int t = blockIdx.x + k * G;
+      if (t >= A.ntiles) break;
+      const int s = k & 1;
+      unsigned char *slot = ring + (size_t)s * C::SLOT_B;
+      const MTile tl = A.tiles[t];
+      const int h0 = A.halo_off[t];
+      const int nh = max(0, min(A.halo_off[t + 1] - h0, kTmHalo));
+      if (lane == 0) {
+        fence_async_smem();
+        const uint32_t hb = (uint32_t)nh * 8u;  // even entry counts: a multiple of 16 bytes
+        mbar_expect_tx(&lst[s], hb);
+        if (hb) bulk_g2s(slot + C::S_HL, A.halo_list + 2 * (int64_t)h0, hb, &lst[s]);
+        kl[s] = k;
+      }
+      bool ok = k < 2 || mbar_wait_bounded(&hfree[s], (uint32_t)((k - 2) >> 1) & 1u, kSpinLimit);
+      ok = ok && mbar_wait_bounded(&lst[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
+      ok = __all_sync(0xffffffffu, ok);
+      if (ok) {
+        // lanes 0-15 and 16-31 take alternate faces, one point per lane, four faces per pass
+        const int32_t *sL = reinterpret_cast<const int32_t *>(slot + C::S_HL);
+        float *sHv = reinterpret_cast<float *>(slot + C::S_HV);
+        const int p = lane & 15;
+        bool gbad = false;
+        if (p < NFP) {
+          for (int i0 = lane >> 4; i0 < nh; i0 += 8) {
+            uint32_t src[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int i = min(i0 + 2 * u, nh - 1);
+              const int2 en = *reinterpret_cast<const int2 *>(sL + 2 * i);
+              src[u] = (uint32_t)en.x + sFt[min(max(en.y, 0), ncodes - 1) * 16 + p];
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const int i = i0 + 2 * u;
+              if (i < nh) {
+                if (src[u] < n_u32)
+                  cp_async4(sHv + i * NFP + p, A.uhi_in + src[u]);
+                else
+                  gbad = true;
+              }
+            }
+          }
         }
-        bulk_commit();
-      };
-      int k = 0;
-      bool bad = false;
-      for (;; ++k) {
-        const int t = blockIdx.x + k * G;
-        if (t >= A.ntiles) break;
-        const int s = k & 1;
+        if (gbad) atomicExch(A.status, kStatusBadGather);
+      }
+      cp_async_arrive_noinc(&full[s]);  // always, so that the fill's phase can complete
+      if (!ok) {
+        bad = true;
+        break;
+      }
+      if (lane == 0) {
         if (k >= 2) {
           if (!mbar_wait_bounded(&done[s], (uint32_t)((k - 2) >> 1) & 1u, kSpinLimit)) {
             bad = true;
-            break;
+          } else {
+            store(s, held[s]);
+            bulk_wait_read_all();  // the slot may be refilled once the stores have read it
           }
-          store(s, held[s]);
-          bulk_wait_read_all();  // the slot may be refilled once the stores have read it
         }
-        if (vload(&sMisc[0])) {
+        if (!bad && vload(&sMisc[0])) bad = true;
+        if (!bad) {
+          held[s] = tl;
+          const uint32_t nb = round16((uint32_t)(tl.nelem * NP * 4));
+          const uint32_t gb = (uint32_t)tl.nelem * kMixedGeoWords * 4;
+          const uint32_t cb = (uint32_t)tl.nelem * 16u;
+          mbar_expect_tx(&full[s], 3 * nb + gb + cb);
+          bulk_g2s(slot, A.uhi_in + tl.node_base, nb, &full[s]);
+          bulk_g2s(slot + C::NODE_B, A.ulo_in + tl.node_base, nb, &full[s]);
+          bulk_g2s(slot + 2 * C::NODE_B, A.resu + tl.node_base, nb, &full[s]);
+          bulk_g2s(slot + C::S_GEO, A.geo + tl.elem_slot * kMixedGeoWords, gb, &full[s]);
+          bulk_g2s(slot + C::S_TC, A.conn + tl.elem_slot * 4, cb, &full[s]);
+          kf[s] = k;
+        }
+      }
+      if (__shfl_sync(0xffffffffu, (int)bad, 0)) {
+        bad = true;
+        break;
+      }
+    }
+    if (!bad && lane == 0) {
+      // the last one or two tiles: write them back once their consumers are done
+      for (int j = (k >= 2 ? k - 2 : 0); j < k && !bad; ++j) {
+        if (!mbar_wait_bounded(&done[j & 1], (uint32_t)(j >> 1) & 1u, kSpinLimit)) {
           bad = true;
           break;
         }
-        const MTile tl = A.tiles[t];
-        held[s] = tl;
-        unsigned char *slot = ring + (size_t)s * C::SLOT_B;
-        const uint32_t nb = round16((uint32_t)(tl.nelem * NP * 4));
-        const uint32_t gb = (uint32_t)tl.nelem * kMixedGeoWords * 4;
-        const uint32_t cb = round16((uint32_t)(tl.nelem * kMixedConnWords * 4));
-        mbar_expect_tx(&full[s], 3 * nb + gb + cb);
-        bulk_g2s(slot, A.uhi_in + tl.node_base, nb, &full[s]);
-        bulk_g2s(slot + C::NODE_B, A.ulo_in + tl.node_base, nb, &full[s]);
-        bulk_g2s(slot + 2 * C::NODE_B, A.resu + tl.node_base, nb, &full[s]);
-        bulk_g2s(slot + 3 * C::NODE_B, A.geo + tl.elem_slot * kMixedGeoWords, gb, &full[s]);
-        bulk_g2s(slot + 3 * C::NODE_B + C::GEO_B, A.conn + tl.elem_slot * kMixedConnWords, cb, &full[s]);
+        store(j & 1, held[j & 1]);
       }
-      if (!bad) {
-        // the last one or two tiles: write them back once their consumers are done
-        for (int j = (k >= 2 ? k - 2 : 0); j < k && !bad; ++j) {
-          if (!mbar_wait_bounded(&done[j & 1], (uint32_t)(j >> 1) & 1u, kSpinLimit)) {
-            bad = true;
-            break;
-          }
-          store(j & 1, held[j & 1]);
-        }
-        bulk_wait_read_all();
-      }
-      if (bad) {
+      bulk_wait_read_all();
+    }
+    if (__shfl_sync(0xffffffffu, (int)bad, 0) || bad) {
+      cp_async_wait_all();
+      if (lane == 0) {
         atomicExch(A.status, kStatusTimeoutCode);
         *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
-        // drain: the newest issued fill of each slot must land before the CTA (and its smem) goes away
-        for (int s = 0; s < 2 && s < k; ++s) {
-          const int kl = s + ((k - 1 - s) >> 1) * 2;
-          mbar_wait_bounded(&full[s], (uint32_t)(kl >> 1) & 1u, kSpinLimit);
+        // drain: the newest list request and fill of each slot must land before the CTA (and its smem) goes
+        for (int s = 0; s < 2; ++s) {
+          if (kl[s] >= 0) mbar_wait_bounded(&lst[s], (uint32_t)(kl[s] >> 1) & 1u, kSpinLimit);
+          if (kf[s] >= 0) mbar_wait_bounded(&full[s], (uint32_t)(kf[s] >> 1) & 1u, kSpinLimit);
         }
         bulk_wait_read_all();
       }
@@ -288,7 +372,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (lane == 0) {
-        split_gemm(tmem, saddr(sA), C::A_PART, saddr(sBV), C::BV_PART, KV, NV, idv);
+        split_gemm(tmem + C::T_ACCV, tmem + C::T_AV, saddr(sBV), C::BV_PART, KV, NV, idv);
         tc_commit(mvol);
       }
       kv = k;
@@ -299,7 +383,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (lane == 0) {
-        split_gemm(tmem + NV, saddr(sA), C::A_PART, saddr(sBL), C::BL_PART, KL, NL, idl);
+        split_gemm(tmem + C::T_ACCL, tmem + C::T_AL, saddr(sBL), C::BL_PART, KL, NL, idl);
         tc_commit(mlift);
       }
       kl = k;
@@ -323,9 +407,6 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
     // b as an unevaluated pair of floats (b = bh + bl to about 2^-48) for the FP32 compensated update
     const float bh = __double2float_rn(A.b), bl = __double2float_rn(A.b - (double)bh);
     const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
-    const int ncodes = A.ncodes;
-    // gathered indices fit 32 bits (the compact connectivity stores int32 bases)
-    const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
     MTile tl_next{};
     if ((int)blockIdx.x < A.ntiles) tl_next = A.tiles[blockIdx.x];
     int k = 0;
@@ -338,51 +419,41 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       const int ne = tl.nelem;
       const bool valid = e < ne;
       const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
-      float *sHi = reinterpret_cast<float *>(ring + (size_t)s * C::SLOT_B);
+      unsigned char *slot = ring + (size_t)s * C::SLOT_B;
+      float *sHi = reinterpret_cast<float *>(slot);
       float *sLo = sHi + TE * NP;
       float *sRe = sLo + TE * NP;
-      const float *sGeo = sRe + TE * NP;
-      const int *sCon = reinterpret_cast<const int *>(sGeo + TE * kMixedGeoWords);
+      const float *sGeo = reinterpret_cast<const float *>(slot + C::S_GEO);
+      const uint32_t *sTc = reinterpret_cast<const uint32_t *>(slot + C::S_TC);
       const int ee = valid ? e : 0;
       const float *hi = sHi + ee * NP;
       const float *lo = sLo + ee * NP;
       const float4 g0 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords);
       const float4 g1 = *reinterpret_cast<const float4 *>(sGeo + ee * kMixedGeoWords + 4);
       const float cr = g0.x, cs = g0.y, ct = g0.z;
-      const int64_t slot0 = tl.node_base, slotn = (int64_t)ne * NP;
+      const int64_t slot0 = tl.node_base;
 
-      // ---- neighbour traces of this thread's faces, loaded first so that their latency overlaps dw ----
+      // ---- neighbour traces of this thread's faces: the slot position of each face's trace (inside the tile,
+      // or the halo) and the face's point order ----
       float fl[FPT][KF];  // uP, then the flux; face h FPT + ff, point p
-      {
-        bool bad = false;
-        const uint32_t codes = (uint32_t)sCon[ee * kMixedConnWords + 4];
 #pragma unroll
-        for (int ff = 0; ff < FPT; ++ff) {
-          const int f = h * FPT + ff;
-          const uint32_t nb = (uint32_t)sCon[ee * kMixedConnWords + f];
-          const int cd = min((int)((codes >> (8 * f)) & 0xffu), ncodes - 1);
-          const uint4 row = *reinterpret_cast<const uint4 *>(sFt + cd * 16);  // this face's point order
-          const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
-          const uint8_t *fm = sFm + f * NFP;
+      for (int ff = 0; ff < FPT; ++ff) {
+        const int f = h * FPT + ff;
+        const uint32_t w = sTc[ee * 4 + f];
+        const int off = (int)(w & 0xffffu);
+        const int cd = min((int)((w >> 16) & 0xffu), ncodes - 1);
+        const uint4 row = *reinterpret_cast<const uint4 *>(sFt + cd * 16);
+        const uint32_t rw[4] = {row.x, row.y, row.z, row.w};
 #pragma unroll
-          for (int p = 0; p < KF; ++p) {
-            float v = 0.f;
-            if (p < NFP && got) {
-              const uint32_t idx = nb + ((rw[p >> 2] >> (8 * (p & 3))) & 0xffu);
-              const uint32_t loc = idx - (uint32_t)slot0;
-              const bool ins = loc < (uint32_t)slotn;
-              const bool okg = idx < n_u32;
-              bad |= valid && !ins && !okg;
-              const float *src = ins ? sHi + loc : (okg ? A.uhi_in + idx : hi + fm[p]);
-              v = *src;
-            }
-            fl[ff][p] = v;
-          }
+        for (int p = 0; p < KF; ++p) {
+          float v = 0.f;
+          if (p < NFP) v = sHi[min(off + (int)((rw[p >> 2] >> (8 * (p & 3))) & 0xffu), C::SLOT_FLOATS - 1)];
+          fl[ff][p] = v;
         }
-        if (bad) atomicExch(A.status, kStatusBadGather);
       }
+      mbar_arrive(&hfree[s]);  // this thread is done with the slot's halo
 
-      // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into three BF16 parts ----
+      // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into TMEM ----
       const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
       const double uC = (double)hi[vC] + (double)lo[vC], uD = (double)hi[vD] + (double)lo[vD];
       const double wA = cons ? 0.5 * uA * uA : uA;
@@ -390,24 +461,22 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       const double dC = (cons ? 0.5 * uC * uC : uC) - wA;
       const double dD = (cons ? 0.5 * uD * uD : uD) - wA;
       const float L0 = (float)(0.5 * ((double)cr * dB + (double)cs * dC + (double)ct * dD));
-      if (got && valid) {
 #pragma unroll
-        for (int c = h; c < KV / 8; c += TPE) {
-          float v[8];
+      for (int c = h; c < KV / 8; c += TPE) {
+        float v[8];
 #pragma unroll
-          for (int q = 0; q < 8; ++q) {
-            const int j = 8 * c + q;
-            v[q] = 0.f;
-            if (j < NP) {
-              const double uj = (double)hi[j] + (double)lo[j];
-              const double wj = cons ? 0.5 * uj * uj : uj;
-              v[q] = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
-            }
+        for (int q = 0; q < 8; ++q) {
+          const int j = 8 * c + q;
+          v[q] = 0.f;
+          if (j < NP) {
+            const double uj = (double)hi[j] + (double)lo[j];
+            const double wj = cons ? 0.5 * uj * uj : uj;
+            v[q] = (float)((wj - wA) - (sBary[3 * j] * dB + sBary[3 * j + 1] * dC + sBary[3 * j + 2] * dD));
           }
-          store_split8(sA + (size_t)kmaj(e, 8 * c, TE) * 2, C::A_PART, v);
         }
+        tmem_split8(lane_tmem + C::T_AV + 4 * c, v);
       }
-      fence_async_smem();  // the A buffer is read by the tensor cores (async proxy)
+      tmem_wait_st();
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(avol);
       if (!got || vload(&sMisc[0])) {
@@ -415,7 +484,8 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
         break;
       }
 
-      // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|) while the MMAs run ----
+      // ---- the Lax-Friedrichs flux 1/2 (uM-uP) (1/2 (uM+uP) g - max(|uM|,|uP|) |g|), into its own TMEM
+      // columns while the volume MMAs run (the LIFT MMAs of the previous tile completed before its update) ----
 #pragma unroll
       for (int ff = 0; ff < FPT; ++ff) {
         const int f = h * FPT + ff;
@@ -427,33 +497,25 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
           const float d = uM - uP;
           fl[ff][p] = 0.5f * d * (0.5f * (uM + uP) * g - fmaxf(fabsf(uM), fabsf(uP)) * ga);
         }
-      }
-
-      // the volume MMAs have read the A buffer (and written acc_V) once mvol completes
-      const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      if (vdone && valid) {
 #pragma unroll
-        for (int ff = 0; ff < FPT; ++ff) {
-          const int f = h * FPT + ff;
+        for (int cq = 0; cq < KF / 8; ++cq) {
+          float v[8];
 #pragma unroll
-          for (int cq = 0; cq < KF / 8; ++cq) {
-            float v[8];
-#pragma unroll
-            for (int q = 0; q < 8; ++q) v[q] = fl[ff][8 * cq + q];
-            store_split8(sA + (size_t)kmaj(e, f * KF + 8 * cq, TE) * 2, C::A_PART, v);
-          }
+          for (int q = 0; q < 8; ++q) v[q] = fl[ff][8 * cq + q];
+          tmem_split8(lane_tmem + C::T_AL + (uint32_t)(f * KF + 8 * cq) / 2, v);
         }
       }
-      fence_async_smem();
+      tmem_wait_st();
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(alift);
+
+      // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
+      const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (!vdone) {
         failed = true;
         break;
       }
-
-      // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
       constexpr int NCE = ((NP + 7) / 8 + TPE - 1) / TPE;  // epilogue chunks per thread
       float t0[NCE][8];
 #pragma unroll
@@ -461,7 +523,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
         const int c = h + TPE * cc;
         if (c < (NP + 7) / 8) {
           float dv[24];  // columns 3i+d of nodes 8c..8c+7
-          tmem_ld24(lane_tmem + 24 * c, dv);
+          tmem_ld24(lane_tmem + C::T_ACCV + 24 * c, dv);
 #pragma unroll
           for (int q = 0; q < 8; ++q) {
             const int i = min(8 * c + q, NP - 1);
@@ -484,7 +546,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
           const int c = h + TPE * cc;
           if (c < (NP + 7) / 8) {
             float lf[8];
-            tmem_ld8(lane_tmem + NV + 8 * c, lf);
+            tmem_ld8(lane_tmem + C::T_ACCL + 8 * c, lf);
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
               const int i = 8 * c + q;
@@ -519,7 +581,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
     }
   }  // consumers
-  // consumers and the MMA warp: TMEM is freed once every load from it and every MMA into it is done
+  // consumers and the MMA warp: TMEM is freed once every access to it and every MMA into it is done
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   asm volatile("bar.sync 1, %0;" ::"n"(32 * (CW + 1)) : "memory");
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -542,7 +604,8 @@ void tcm_attr() {
 
 template <int N, int CW, bool CONS>
 bool launch_tcm_n(const MixedArgs &A, int num_sms, cudaStream_t st, LaunchInfo *info) {
-  const uint32_t smem = tm_smem<N>(A.ncodes);
+  // at least 116 KB of shared memory, so that one CTA (which holds all 512 TMEM columns) runs per SM
+  const uint32_t smem = std::max<uint32_t>(tm_smem<N>(A.ncodes), 116u * 1024u);
   if (smem > 227u * 1024u) return false;
   tcm_attr<N, CW, CONS>();
   const int grid = std::max(1, std::min(num_sms, A.ntiles));
@@ -600,6 +663,18 @@ void tcm_pack_n(const double *Dr, const double *Ds, const double *Dt, const doub
 }  // namespace
 
 int tcm_tile_elems() { return kTmTE; }
+
+int tcm_halo_capacity() { return kTmHalo; }
+
+int tcm_halo_floats(int N) {
+  switch (N) {
+    case 1: return TmCfg<1>::HALO_FLOATS;
+    case 2: return TmCfg<2>::HALO_FLOATS;
+    case 3: return TmCfg<3>::HALO_FLOATS;
+    case 4: return TmCfg<4>::HALO_FLOATS;
+    default: return 0;
+  }
+}
 
 bool tcm_supported(int N) { return N >= 1 && N <= 4; }
 

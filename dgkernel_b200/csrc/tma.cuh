@@ -72,6 +72,17 @@ __device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bu
 // Makes this thread's generic-proxy shared-memory writes visible to later bulk copies (async proxy).
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// 4-byte asynchronous global -> shared copy (no registers held while it is in flight).
+__device__ __forceinline__ void cp_async4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+// Arrive on `bar` once every cp.async this thread issued so far has completed; the arrival counts towards the
+// barrier's expected count (its init count includes one per arriving thread).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t *bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(saddr(bar)) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 constexpr uint32_t kSpinLimit = 1u << 26;  // polls; a healthy stage completes in microseconds
 
 __host__ __device__ constexpr uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }

@@ -116,6 +116,29 @@ def compact_faces(Kpart, node_off, face_off, Np, Nfp, gmap):
     return conn[:slots * 5].reshape(slots, 5), table[:nc.value * Nfp].reshape(nc.value, Nfp)
 
 
+def tile_halo(Kpart, node_off, Np, Nfp, conn, max_elems=128, max_halo=256, halo_floats=None, identity_code=255,
+              align=4):
+    """Tiles of the tensor-core mixed stage with their halos (dgk_tile_halo): dict with part, first, nelem,
+    halo_off, halo_list ([entries, 2] int32) and tconn ([slots, 4] uint32)."""
+    K = np.ascontiguousarray(Kpart, dtype=np.int64)
+    no = np.ascontiguousarray(node_off, dtype=np.int64)
+    cn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1)
+    hf = max_elems * Np if halo_floats is None else halo_floats
+    counts = np.zeros(2, dtype=np.int64)
+    args = (len(K), _p(K, _PI64), _p(no, _PI64), Np, Nfp, _p(cn, _PI32), max_elems, max_halo, hf, identity_code,
+            align, _p(counts, _PI64))
+    check(lib().dgk_tile_halo(*args, None, None, None, None, None, None))
+    nt, nh = int(counts[0]), int(counts[1])
+    part, nelem, hoff = (np.zeros(nt + (i == 2), dtype=np.int32) for i in range(3))
+    first = np.zeros(nt, dtype=np.int64)
+    hl = np.zeros(max(2 * nh, 2), dtype=np.int32)
+    tc = np.zeros(max(cn.size // 5 * 4, 4), dtype=np.uint32)
+    check(lib().dgk_tile_halo(*args, _p(part, _PI32), _p(first, _PI64), _p(nelem, _PI32), _p(hoff, _PI32),
+                              _p(hl, _PI32), tc.ctypes.data_as(C.POINTER(C.c_uint32))))
+    return {"part": part, "first": first, "nelem": nelem, "halo_off": hoff, "halo_list": hl[:2 * nh].reshape(nh, 2),
+            "tconn": tc[:cn.size // 5 * 4].reshape(-1, 4)}
+
+
 def splitmix_uniform(seed: int, count: int) -> np.ndarray:
     out = np.zeros(count)
     check(lib().dgk_splitmix_uniform(seed, count, _p(out, _PD)))

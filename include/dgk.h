@@ -212,6 +212,20 @@ int dgk_face_gather_map(int64_t K, int32_t Nfaces, int32_t Nfp, int32_t Np, cons
 int dgk_compact_faces(int32_t npart, const int64_t *K, const int64_t *node_off, const int64_t *face_off,
                       int32_t Np, int32_t Nfp, const int32_t *gmap, int32_t *conn_out, uint8_t *table_out,
                       int32_t table_cap, int32_t *ncodes_out);
+/* Tiles of the tensor-core mixed stage (rhsStageMixed mma=1) with their halos, from the compact connectivity
+ * above (conn in dgk_compact_faces' slot layout).  Each partition is cut into runs of consecutive elements of
+ * at most max_elems, starting on multiples of `align`, with at most max_halo (even) faces whose neighbour lies
+ * outside the run.  Call once with the output pointers NULL to get counts_out = {tiles, halo entries}, then
+ * again with room for them: per tile part_out, first_out (partition-local first element), nelem_out,
+ * halo_off_out (tiles + 1, in entries); halo_list_out holds (neighbour base, code) int32 pairs, each tile's
+ * list padded to an even count by repeating its last entry; tconn_out (4 per element slot) = the neighbour
+ * trace's position in the tile's shared-memory slot (low 16 bits, floats: (neighbour - first) * Np inside
+ * the tile, halo_floats + j * Nfp for halo face j) | code << 16 (identity_code for halo faces).  Derived from
+ * the FaceConnector lists (utils/face_connector.go:143-205); the reference has no tiled form. */
+int dgk_tile_halo(int32_t npart, const int64_t *K, const int64_t *node_off, int32_t Np, int32_t Nfp,
+                  const int32_t *conn, int32_t max_elems, int32_t max_halo, int32_t halo_floats, int32_t identity_code,
+                  int32_t align, int64_t *counts_out, int32_t *part_out, int64_t *first_out, int32_t *nelem_out,
+                  int32_t *halo_off_out, int32_t *halo_list_out, uint32_t *tconn_out);
 
 /* GPU FP64 setup (element/library/gonudg/startup3d.go:121-148, normals3d.go:11-207,
  * buildmaps3d.go:5-153) into the runner's bound arrays.  names[] lists the target binding for each of

@@ -214,6 +214,27 @@ def test_matmul_operator(c1):
     r.Free()
 
 
+def test_matmul_add_operator(c1):
+    # MATMUL_ADD_<M> (runner/builder/builder.go:355-410): OUT += M x IN per element, OUT starting nonzero
+    el, K, Np = c1.el, c1.Kpart, c1.el.Np
+    U = split(np.ascontiguousarray(c1.u0.reshape(-1)), K, Np)
+    start = np.random.default_rng(11).standard_normal(c1.K * Np)
+    out = split(start.copy(), K, Np)
+    r = Runner(Config(K=K))
+    r.DefineBindings(Input("Ds_NudgTet2").Bind(el.Ds).ToMatrix().Static(), Input("U").Bind(U),
+                     InOut("Us").Bind(out))
+    r.AllocateDevice()
+    r.ConfigureKernel("mma", r.Param("U").CopyTo(), r.Param("Us").Copy(), r.Param("Ds_NudgTet2"))
+    r.BuildKernel("matmulAdd(M=Ds_NudgTet2,IN=U,OUT=Us)", "mma")
+    r.ExecuteKernel("mma")
+    off = np.concatenate(([0], np.cumsum(np.array(K) * Np))).astype(np.int64)
+    want = start.copy()
+    O.lib().ora_matmul(O.cm(el.Ds), Np, Np, len(K), np.array(K, dtype=np.int64),
+                       np.ascontiguousarray(c1.u0.reshape(-1)), off, want, off, 1)
+    assert rel_l2(np.concatenate(out), want) < FP64_TOL
+    r.Free()
+
+
 def test_copy_engine_conversions_and_transposes():
     K = [3, 5]
     rng = np.random.default_rng(7)
