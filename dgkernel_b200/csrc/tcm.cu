@@ -16,19 +16,19 @@
 // a product keeps the six terms a_p b_q with p + q <= 2, all accumulated in one FP32 TMEM accumulator: the
 // products carry FP32-level rounding (the dropped terms are below 2^-24 of the product).
 //
-// CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry and tile-local
-// connectivity into a 2-slot ring with 1-D bulk copies, gathers the tile's halo (the traces of neighbours
-// outside the tile, listed per tile by the host) into the slot with 4-byte asynchronous copies, and writes
-// finished slots back with bulk stores; one MMA warp issues the GEMMs with operand A read from tensor memory
-// and operand B (D and LIFT, split) from shared memory, where it stays for the whole launch; CW consumer warps
-// hold CW / 4 threads per element (warps w, w + 4, ... share the TMEM lane quarter w mod 4 and split the
-// element's nodes in 8-wide chunks and its faces).  Per tile: the consumer threads read their faces'
-// neighbour traces from the slot (inside the tile, or the halo), store the split dw into TMEM and arrive on
-// an mbarrier, on which the MMA warp issues the volume GEMM; they form the flux meanwhile, store it into its
-// own TMEM columns and arrive again for the LIFT GEMM; then they read both accumulators and finish the stage
-// (the compensated update in error-free FP32 arithmetic) into the slot.  No barrier among the consumers within
-// a tile.  Every wait is bounded; a failed wait sets the status word and the CTA leaves after draining its
-// copies and MMAs; TMEM is always freed.
+// CTA: one producer warp streams each tile's state (hi, lo, resu), compact geometry, tile-local connectivity
+// and halo list (the faces whose neighbour lies outside the tile, listed per tile by the host) into a 2-slot
+// ring with 1-D bulk copies and writes finished slots back with bulk stores; one MMA warp issues the GEMMs
+// with operand A read from tensor memory and operand B (D and LIFT, split) from shared memory, where it stays
+// for the whole launch; CW consumer warps hold CW / 4 threads per element (warps w, w + 4, ... share the TMEM
+// lane quarter w mod 4 and split the element's nodes in 8-wide chunks and its faces).  Per tile: the consumer
+// threads read their faces' neighbour traces from the slot (inside the tile, or the halo), store the split dw
+// into TMEM and arrive on an mbarrier, on which the MMA warp issues the volume GEMM; they form the flux
+// meanwhile, store it into its own TMEM columns and arrive again for the LIFT GEMM; while the MMAs run they
+// gather the next tile's halo values into the other slot with 4-byte asynchronous copies (a few per thread);
+// then they read both accumulators and finish the stage (the compensated update in error-free FP32
+// arithmetic) into the slot.  No barrier among the consumers within a tile.  Every wait is bounded; a failed
+// wait sets the status word and the CTA leaves after draining its copies and MMAs; TMEM is always freed.
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -69,7 +69,7 @@ struct TmCfg {
   // shared-memory layout (bytes)
   static constexpr uint32_t OFF_BV = 0, OFF_BL = OFF_BV + 3 * BV_PART, OFF_SLOT = OFF_BL + 3 * BL_PART;
   static constexpr uint32_t OFF_BARY = OFF_SLOT + 2 * SLOT_B;
-  // full[2], done[2], mvol, mlift, avol, alift, lst[2], hfree[2]
+  // full[2], done[2], mvol, mlift, avol, alift, lst[2], hful[2]
   static constexpr uint32_t OFF_BARS = OFF_BARY + (uint32_t)NP * 3 * 8;
   static constexpr uint32_t OFF_MISC = OFF_BARS + 12 * 8;  // abort flag, TMEM base
   static constexpr uint32_t OFF_FMASK = (OFF_MISC + 16 + 15) & ~15u;
@@ -179,12 +179,11 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
   unsigned char *sBV = sm + C::OFF_BV, *sBL = sm + C::OFF_BL;
   unsigned char *ring = sm + C::OFF_SLOT;
   double *sBary = reinterpret_cast<double *>(sm + C::OFF_BARY);
-  // full: slot filled (the producer's bulk copies, and every producer lane's halo copies); done: slot finished
-  // (every consumer thread); mvol / mlift: MMA group complete (tcgen05.commit); avol / alift: operand written
-  // into TMEM (every consumer thread); lst: a slot's halo list arrived; hfree: every consumer thread has read
-  // the slot's halo
+  // full: slot filled (the producer's bulk copies); done: slot finished (every consumer thread); mvol / mlift:
+  // MMA group complete (tcgen05.commit); avol / alift: operand written into TMEM (every consumer thread); lst:
+  // a slot's halo list arrived; hful: a slot's halo values arrived (every consumer thread's copies)
   uint64_t *full = reinterpret_cast<uint64_t *>(sm + C::OFF_BARS), *done = full + 2, *mvol = full + 4,
-           *mlift = full + 5, *avol = full + 6, *alift = full + 7, *lst = full + 8, *hfree = full + 10;
+           *mlift = full + 5, *avol = full + 6, *alift = full + 7, *lst = full + 8, *hful = full + 10;
   int *sMisc = reinterpret_cast<int *>(sm + C::OFF_MISC);  // [0] abort flag, [1] TMEM base
   uint8_t *sFm = sm + C::OFF_FMASK, *sFt = sm + C::OFF_FTAB;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -201,7 +200,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
   for (int x = tid; x < NF; x += blockDim.x) sFm[x] = (uint8_t)A.fmask[x];
   for (int x = tid; x < ncodes * 16; x += blockDim.x) sFt[x] = (x & 15) < NFP ? A.ftab[(x >> 4) * NFP + (x & 15)] : 0;
   if (tid == 0) {
-    for (int b = 0; b < 2; ++b) mbar_init(&full[b], 1 + 32);  // the bulk copies' arrival and 32 producer lanes
+    for (int b = 0; b < 2; ++b) mbar_init(&full[b], 1);
     for (int b = 2; b < 4; ++b) mbar_init(&full[b], 32 * CW);
     mbar_init(mvol, 1);
     mbar_init(mlift, 1);
@@ -209,8 +208,8 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
     mbar_init(alift, 32 * CW);
     mbar_init(&lst[0], 1);
     mbar_init(&lst[1], 1);
-    mbar_init(&hfree[0], 32 * CW);
-    mbar_init(&hfree[1], 32 * CW);
+    mbar_init(&hful[0], 32 * CW);
+    mbar_init(&hful[1], 32 * CW);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     sMisc[0] = 0;
   }
@@ -226,16 +225,14 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
   const uint32_t tmem = (uint32_t)sMisc[1];
 
   if (warp == CW + 1) {
-    // producer warp.  Slot s holds tile k, then k + 2.  Per tile: lane 0 requests the tile's halo list (only
-    // this warp reads the list region, and it has finished with tile k - 2's); once every consumer thread has
-    // read tile k - 2's halo (hfree[s]) and the list has landed, every lane gathers its share of the halo values
-    // with 4-byte asynchronous copies and arrives on full[s] when they have landed.  Then lane 0 waits until
-    // every consumer thread has finished tile k - 2 (done[s]), writes its hi, lo and resu out with bulk stores
-    // (the ragged tail past the last full 16 bytes was written by the consumers) and refills the slot once the
-    // stores have read it.
+    // producer warp, lane 0.  Slot s holds tile k, then k + 2.  Per tile: wait until every consumer thread has
+    // finished tile k - 2 (done[s]), write its hi, lo and resu out with bulk stores (the ragged tail past the
+    // last full 16 bytes was written by the consumers) and refill the slot once the stores have read it.  The
+    // consumers read tile j's halo list while they work on tile j - 1 (tile 0's before their first tile), so
+    // list j may replace list j - 2 once tile j - 3 is done: lists 0 and 1 go first, lists 2 and 3 after tile
+    // 0 is done, list k + 1 after tile k - 2 is done.
     MTile held[2] = {};
-    int kl[2] = {-1, -1}, kf[2] = {-1, -1};  // newest list request and newest fill of each slot (lane 0)
-    const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
+    int kl[2] = {-1, -1}, kf[2] = {-1, -1};  // newest list request and newest fill of each slot
     auto store = [&](int s, const MTile &tl) {
       const uint32_t nbd = (((uint32_t)(tl.nelem * NP * 4)) & ~15u);
       unsigned char *slot = ring + (size_t)s * C::SLOT_B;
@@ -246,6 +243,16 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       }
       bulk_commit();
     };
+    auto request_list = [&](int kk) {
+      const int tt = blockIdx.x + kk * G;
+      if (tt >= A.ntiles) return;
+      const int h0 = A.halo_off[tt];
+      const int nh = max(0, min(A.halo_off[tt + 1] - h0, kTmHalo));
+      const uint32_t hb = (uint32_t)nh * 8u;  // even entry counts: a multiple of 16 bytes
+      mbar_expect_tx(&lst[kk & 1], hb);
+      if (hb) bulk_g2s(ring + (size_t)(kk & 1) * C::SLOT_B + C::S_HL, A.halo_list + 2 * (int64_t)h0, hb, &lst[kk & 1]);
+      kl[kk & 1] = kk;
+    };
     int k = 0;
     bool bad = false;
     for (;; ++k) {
@@ -254,52 +261,6 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       const int s = k & 1;
       unsigned char *slot = ring + (size_t)s * C::SLOT_B;
       const MTile tl = A.tiles[t];
-      const int h0 = A.halo_off[t];
-      const int nh = max(0, min(A.halo_off[t + 1] - h0, kTmHalo));
-      if (lane == 0) {
-        fence_async_smem();
-        const uint32_t hb = (uint32_t)nh * 8u;  // even entry counts: a multiple of 16 bytes
-        mbar_expect_tx(&lst[s], hb);
-        if (hb) bulk_g2s(slot + C::S_HL, A.halo_list + 2 * (int64_t)h0, hb, &lst[s]);
-        kl[s] = k;
-      }
-      bool ok = k < 2 || mbar_wait_bounded(&hfree[s], (uint32_t)((k - 2) >> 1) & 1u, kSpinLimit);
-      ok = ok && mbar_wait_bounded(&lst[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
-      ok = __all_sync(0xffffffffu, ok);
-      if (ok) {
-        // lanes 0-15 and 16-31 take alternate faces, one point per lane, four faces per pass
-        const int32_t *sL = reinterpret_cast<const int32_t *>(slot + C::S_HL);
-        float *sHv = reinterpret_cast<float *>(slot + C::S_HV);
-        const int p = lane & 15;
-        bool gbad = false;
-        if (p < NFP) {
-          for (int i0 = lane >> 4; i0 < nh; i0 += 8) {
-            uint32_t src[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int i = min(i0 + 2 * u, nh - 1);
-              const int2 en = *reinterpret_cast<const int2 *>(sL + 2 * i);
-              src[u] = (uint32_t)en.x + sFt[min(max(en.y, 0), ncodes - 1) * 16 + p];
-            }
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              const int i = i0 + 2 * u;
-              if (i < nh) {
-                if (src[u] < n_u32)
-                  cp_async4(sHv + i * NFP + p, A.uhi_in + src[u]);
-                else
-                  gbad = true;
-              }
-            }
-          }
-        }
-        if (gbad) atomicExch(A.status, kStatusBadGather);
-      }
-      cp_async_arrive_noinc(&full[s]);  // always, so that the fill's phase can complete
-      if (!ok) {
-        bad = true;
-        break;
-      }
       if (lane == 0) {
         if (k >= 2) {
           if (!mbar_wait_bounded(&done[s], (uint32_t)((k - 2) >> 1) & 1u, kSpinLimit)) {
@@ -311,6 +272,12 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
         }
         if (!bad && vload(&sMisc[0])) bad = true;
         if (!bad) {
+          if (k == 0 || k == 2) {
+            request_list(k);
+            request_list(k + 1);
+          } else if (k >= 3) {
+            request_list(k + 1);
+          }
           held[s] = tl;
           const uint32_t nb = round16((uint32_t)(tl.nelem * NP * 4));
           const uint32_t gb = (uint32_t)tl.nelem * kMixedGeoWords * 4;
@@ -341,7 +308,6 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       bulk_wait_read_all();
     }
     if (__shfl_sync(0xffffffffu, (int)bad, 0) || bad) {
-      cp_async_wait_all();
       if (lane == 0) {
         atomicExch(A.status, kStatusTimeoutCode);
         *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
@@ -407,10 +373,42 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
     // b as an unevaluated pair of floats (b = bh + bl to about 2^-48) for the FP32 compensated update
     const float bh = __double2float_rn(A.b), bl = __double2float_rn(A.b - (double)bh);
     const int vA = A.vtx[0], vB = A.vtx[1], vC = A.vtx[2], vD = A.vtx[3];
+    const uint32_t n_u32 = (uint32_t)min(A.n_u_values, (int64_t)0xffffffffu);
+    // halo values of this CTA's tile kk into its slot: value v of the tile's halo (face v / NFP, point v mod
+    // NFP, in the face's point order) is this thread's when v = tid mod 32 CW; every consumer thread arrives on
+    // hful once its copies have landed
+    auto gather_halo = [&](int kk) -> bool {
+      const int tt = blockIdx.x + kk * G, ss = kk & 1;
+      unsigned char *sl = ring + (size_t)ss * C::SLOT_B;
+      const int h0 = A.halo_off[tt];
+      const int nv = max(0, min(A.halo_off[tt + 1] - h0, kTmHalo)) * NFP;
+      const bool ok = mbar_wait_bounded(&lst[ss], (uint32_t)(kk >> 1) & 1u, kSpinLimit);
+      if (ok) {
+        const int32_t *sL = reinterpret_cast<const int32_t *>(sl + C::S_HL);
+        float *sHv = reinterpret_cast<float *>(sl + C::S_HV);
+        bool gbad = false;
+#pragma unroll 2
+        for (int v = tid; v < nv; v += 32 * CW) {
+          const int i = v / NFP, p = v - i * NFP;
+          const int2 en = *reinterpret_cast<const int2 *>(sL + 2 * i);
+          const uint32_t src = (uint32_t)en.x + sFt[min(max(en.y, 0), ncodes - 1) * 16 + p];
+          if (src < n_u32)
+            cp_async4(sHv + v, A.uhi_in + src);
+          else
+            gbad = true;
+        }
+        if (gbad) atomicExch(A.status, kStatusBadGather);
+      }
+      cp_async_arrive_noinc(&hful[ss]);  // always, so that the phase can complete
+      return ok;
+    };
     MTile tl_next{};
-    if ((int)blockIdx.x < A.ntiles) tl_next = A.tiles[blockIdx.x];
+    if ((int)blockIdx.x < A.ntiles) {
+      tl_next = A.tiles[blockIdx.x];
+      if (!gather_halo(0)) failed = true;
+    }
     int k = 0;
-    for (;; ++k) {
+    for (; !failed; ++k) {
       const int t = blockIdx.x + k * G;
       if (t >= A.ntiles) break;
       const int s = k & 1;
@@ -418,7 +416,8 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       if (t + G < A.ntiles) tl_next = A.tiles[t + G];  // the next descriptor's load overlaps this tile
       const int ne = tl.nelem;
       const bool valid = e < ne;
-      const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
+      const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit) &&
+                       mbar_wait_bounded(&hful[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
       unsigned char *slot = ring + (size_t)s * C::SLOT_B;
       float *sHi = reinterpret_cast<float *>(slot);
       float *sLo = sHi + TE * NP;
@@ -451,7 +450,6 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
           fl[ff][p] = v;
         }
       }
-      mbar_arrive(&hfree[s]);  // this thread is done with the slot's halo
 
       // ---- volume operand: dw = w - P1(w), this thread's 8-column chunks of K, split into TMEM ----
       const double uA = (double)hi[vA] + (double)lo[vA], uB = (double)hi[vB] + (double)lo[vB];
@@ -508,6 +506,11 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       tmem_wait_st();
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       mbar_arrive(alift);
+      // the next tile's halo, while the MMAs run (its slot's previous halo was read before tile k - 1's LIFT)
+      if (t + G < A.ntiles && !gather_halo(k + 1)) {
+        failed = true;
+        break;
+      }
 
       // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
       const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
@@ -576,6 +579,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       fence_async_smem();  // the slot writes become visible to the producer's bulk stores
       mbar_arrive(&done[s]);
     }
+    cp_async_wait_all();  // no halo copy may land after the CTA has gone
     if (failed && lane == 0) {
       atomicExch(A.status, kStatusTimeoutCode);
       *reinterpret_cast<volatile int *>(&sMisc[0]) = 1;
