@@ -60,6 +60,29 @@ def b_alg_mixed(N: int) -> float:
     return 6 * 4 + (8 * 4 + 5 * 4) / Np
 
 
+def b_alg_tcm(N: int, halo_per_elem: float) -> float:
+    """Algorithmic bytes per DOF-stage of the tensor-core mixed stage: hi, lo and resu read and written (FP32),
+    the compact per-element geometry (8 floats), the tile-local connectivity (4 int32) and the tile's halo list
+    (8 bytes per face whose neighbour lies outside the tile), spread over the Np nodes."""
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    return 6 * 4 + (8 * 4 + 4 * 4 + 8 * halo_per_elem) / Np
+
+
+def kuhn_halo_per_elem(n: int, slabs: int, tile: int = 128) -> float:
+    """Faces per element whose neighbour lies outside the element's tile (tiles of `tile` consecutive elements
+    of one x-slab partition) on the periodic n^3 x 6 Kuhn mesh: the halo the tensor-core stage gathers."""
+    from dgkernel_b200 import mesh as M
+    _, _, _, _, EToVp, EToP = M.kuhn_mesh(n, slabs)
+    EToE, _ = M.ti_connect3d(EToVp)
+    K = EToE.shape[0]
+    Kp = K // slabs
+    e = np.arange(K)
+    first = (e // Kp) * Kp + ((e % Kp) // tile) * tile  # first element of each element's tile
+    last = np.minimum(first + tile, (e // Kp + 1) * Kp)
+    outside = (EToE < first[:, None]) | (EToE >= last[:, None])
+    return float(outside.sum()) / K
+
+
 def b_alg_per_dof(N: int, elem_bytes: int) -> float:
     """Algorithmic bytes per DOF-stage of the fused stage kernel in the reference-contract layout:
     u read + resu read + resu write + u write, 9 per-node metrics, and per face point nx, ny, nz, Fscale plus
@@ -577,7 +600,8 @@ def run_burgers(args, world, rank, local):
         ms = max_over_ranks(ms, world)
         finals[name] = prob.get("u").astype(np.float64)
         results[name] = {"ms": ms, "dofs": prob.dofs, "clocks": clk.summary(), "prob": prob,
-                         "b_alg": b_alg_mixed(args.order) if name.startswith("mixed") else
+                         "b_alg": b_alg_tcm(args.order, kuhn_halo_per_elem(args.n, args.slabs))
+                         if name == "mixed_tc" else b_alg_mixed(args.order) if name == "mixed" else
                          b_alg_per_dof(args.order, 8 if name == "f64" else 4),
                          "kernel": kernels[name]}
         if name != "f64":
