@@ -2,14 +2,17 @@
 // the BR1 viscous term only where it is not zero.
 //
 // Per stage, before the tensor-core mixed stage (tcm.cu), which adds the result to its right-hand side:
-//   ls_sensor   every element: modal coefficients uhat = Vinv u (FP64), the Persson-Peraire activation from
-//               log10(E_top / E), the 35 -> 32 -> 32 -> 1 network (tanh, tanh, sigmoid; FP16 weights, FP32 sums)
-//               on uhat / |uhat| with the PP fallback inside (lo, hi) and, in mode 3, outputs <= lo read as a
-//               smooth element; eps_e = eps0 sigma_e h_e / N; elements with eps_e > 0 form the active list.
+//   ls_sensor   every element: modal coefficients uhat = Vinv u (FP64, on the FP64 tensor path), the
+//               Persson-Peraire activation from log10(E_top / E), the 35 -> 32 -> 32 -> 1 network (tanh, tanh,
+//               sigmoid; FP16 weights, FP32 sums) on uhat / |uhat| with the PP fallback inside (lo, hi) and, in
+//               mode 3, outputs <= lo read as a smooth element; eps_e = eps0 sigma_e h_e / N; elements with
+//               eps_e > 0 form the active list.
 //   ls_touch    the active elements and their face neighbours are marked; ls_compact lists them (touched).
-//   ls_grad     active elements: q_d = D_d u + LIFT (Fscale n_d (uP - uM) / 2) (FP64), stored as eps_e q_d.
-//   ls_div      touched elements: eps_e sum_d D_d q_d + LIFT (Fscale / 2 sum_d n_d (epsP qP_d - epsM qM_d)),
-//               the viscous right-hand side, with eps q = 0 on elements that are not active.
+//   ls_grad     active elements: q_d = D_d u + LIFT (Fscale n_d (uP - uM) / 2) (FP64 tensor path), stored as
+//               eps_e q_d.
+//   ls_div      touched elements: sum_d d/dx_d (eps_e q_d) + LIFT (Fscale / 2 sum_d n_d (epsP qP_d - epsM qM_d)),
+//               the viscous right-hand side, with eps q = 0 on elements that are not active; on straight-sided
+//               elements the derivative is sum_k D_k (sum_d (d xi_k / d x_d) eps q_d) (FP64 tensor path).
 // This is the BR1 viscosity of the plain viscosity stage (av.cu) restricted to where it is not zero: an element
 // whose own and neighbours' eps vanish gets no viscous term there either.  The sparse passes walk device-side
 // counts with persistent grids, so a stage needs no host synchronisation.
@@ -80,15 +83,68 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
   __syncthreads();
   const __half *W1 = sW, *b1 = W1 + kLsHid * NP, *W2 = b1 + kLsHid, *b2 = W2 + kLsHid * kLsHid, *w3 = b2 + kLsHid,
                *b3 = w3 + kLsHid;
-  for (int st = blockIdx.x; st < 2 * A.ntiles; st += gridDim.x) {
+  // the state of the block's next 64 elements is loaded into registers while the current ones are computed
+  constexpr int FILL = (kLsElems * NP + 4 * kLsElems - 1) / (4 * kLsElems);  // values per thread
+  float fh[FILL], fl[FILL];
+  auto load = [&](int st) {
     const MTile tl = A.tiles[st >> 1];
     const int e0 = (st & 1) * kLsElems;  // half of the 128-element tile
     const int ne = max(0, min(kLsElems, tl.nelem - e0));
     const int64_t base = tl.node_base + (int64_t)e0 * NP;
-    for (int x = tid; x < ne * NP; x += blockDim.x) su[x] = (double)A.uhi[base + x] + (double)A.ulo[base + x];
+#pragma unroll
+    for (int q = 0; q < FILL; ++q) {
+      const int x = tid + q * 4 * kLsElems;
+      fh[q] = x < ne * NP ? A.uhi[base + x] : 0.f;
+      fl[q] = x < ne * NP ? A.ulo[base + x] : 0.f;
+    }
+  };
+  if ((int)blockIdx.x < 2 * A.ntiles) load(blockIdx.x);
+  for (int st = blockIdx.x; st < 2 * A.ntiles; st += gridDim.x) {
+    const MTile tl = A.tiles[st >> 1];
+    const int e0 = (st & 1) * kLsElems;  // half of the 128-element tile
+    const int ne = max(0, min(kLsElems, tl.nelem - e0));
+#pragma unroll
+    for (int q = 0; q < FILL; ++q) {
+      const int x = tid + q * 4 * kLsElems;
+      if (x < kLsElems * NP) su[x] = (double)fh[q] + (double)fl[q];
+    }
     __syncthreads();
+    if (st + (int)gridDim.x < 2 * A.ntiles) load(st + gridDim.x);
     const bool valid = e < ne;
-    const double *ue = su + (valid ? e : 0) * NP;
+    // modal coefficients uhat = Vinv u of this warp's 8 elements on the FP64 tensor path (mma.sync m8n8k4):
+    // A = Vinv (8-row m-tiles, 4-column k-steps), B = the elements' nodal values (one element per column);
+    // they overwrite the warp's own rows of su
+    {
+      constexpr int MT = (NP + 7) / 8, KT = (NP + 3) / 4;
+      const int lane = tid & 31, w0 = (tid >> 5) * 8;
+      const int ar = lane >> 2, ac = lane & 3, be = w0 + (lane >> 2);
+      double c[MT][2];
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) c[mt][0] = c[mt][1] = 0.0;
+#pragma unroll
+      for (int kk = 0; kk < KT; ++kk) {
+        const int j = 4 * kk + ac;
+        const double bv = (j < NP && be < ne) ? su[be * NP + j] : 0.0;
+#pragma unroll
+        for (int mt = 0; mt < MT; ++mt) {
+          const int r = 8 * mt + ar;
+          const double av = (r < NP && j < NP) ? sVi[r * NP + j] : 0.0;
+          asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                       : "+d"(c[mt][0]), "+d"(c[mt][1])
+                       : "d"(av), "d"(bv));
+        }
+      }
+      __syncwarp();  // every lane's reads of the nodal values are done
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const int r = 8 * mt + ar;
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (r < NP) su[(w0 + 2 * ac + h) * NP + r] = c[mt][h];
+      }
+      __syncwarp();
+    }
+    const double *ue = su + (valid ? e : 0) * NP;  // now the element's modal coefficients
     double tot = 0.0, top = 0.0;
     double uh[(NP + 3) / 4];
 #pragma unroll
@@ -96,8 +152,7 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
       const int i = t + 4 * k;
       double s = 0.0;
       if (i < NP) {
-#pragma unroll 5
-        for (int j = 0; j < NP; ++j) s = fma(sVi[i * NP + j], ue[j], s);
+        s = ue[i];
         tot = fma(s, s, tot);
         if (sTop[i]) top = fma(s, s, top);
       }
@@ -197,122 +252,256 @@ __global__ void ls_compact_kernel(const LsArgs A) {
   }
 }
 
-// Sparse passes: one warp per element, lanes over the element's nodes (i = lane, lane + 32) and face points; the
-// FP64 matrices are read transposed from global memory (DT[j][i], LT[m][i]: a warp's lanes read consecutive
-// values, and the few tens of KB stay in L1), per-warp values in shared memory, no block barrier.
-constexpr int kLsWarps = 8;  // warps (elements in flight) per block
+// Sparse passes: one block of MT warps per group of 8 listed elements (the n-tile of the FP64 tensor path,
+// mma.sync m8n8k4).  The block stages the group in shared memory (per-element offsets, eps and metrics; nodal
+// values; face terms: each thread's few face points with their loads issued together), then warp mt applies the
+// element matrices to rows 8 mt .. 8 mt + 7, reading their fragments transposed through L1 (DT[j][i], LT[m][i]:
+// the few tens of KB stay there); lane l's output row is 8 mt + l / 4, its elements 2 (l mod 4) and
+// 2 (l mod 4) + 1.  The mixed stage requires straight-sided elements, so the metrics are constant over an
+// element and are read once per element.
+__device__ __forceinline__ void ls_dmma(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
 
 template <int N>
-__global__ void __launch_bounds__(32 * kLsWarps) ls_grad_kernel(const LsArgs A) {
+struct LsCfg {
   using O = Order<N>;
-  constexpr int NP = O::NP, NF = O::NF;
-  __shared__ double s_u[kLsWarps][NP], s_j[kLsWarps][3][NF];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double *su = s_u[w];
-  const int n = *reinterpret_cast<volatile const int *>(&A.counts[0]);
-  for (int a = blockIdx.x * kLsWarps + w; a < n; a += gridDim.x * kLsWarps) {
-    const int64_t slot = A.alist[a];
-    const int p = part_of_slot(A, slot);
-    const int64_t le = slot - A.slot_prefix[p];
-    const int64_t ub = A.uoff[p] + le * NP, gb = A.goff[p] + le * NP, fb = A.foff[p] + le * NF;
-    for (int i = lane; i < NP; i += 32) su[i] = (double)A.uhi[ub + i] + (double)A.ulo[ub + i];
-    __syncwarp();
-    for (int m = lane; m < NF; m += 32) {
-      const int32_t g = A.gmap[fb + m];
-      const double uM = su[A.fmask[m]];
-      double uP = uM;
-      if ((uint64_t)(int64_t)g < (uint64_t)A.n_u_values) {
-        uP = (double)A.uhi[g] + (double)A.ulo[g];
-      } else {
-        atomicExch(A.status, kStatusBadGather);
-      }
-      const double jump = 0.5 * (uP - uM) * A.face[3][fb + m];
-      for (int d = 0; d < 3; ++d) s_j[w][d][m] = A.face[d][fb + m] * jump;
+  static constexpr int NP = O::NP, NF = O::NF;
+  static constexpr int MT = (NP + 7) / 8, KT = (NP + 3) / 4, KL = NF / 4;
+  static constexpr int NPU = 4 * KT;  // padded node rows of a staged element
+  static constexpr int THREADS = 32 * MT;
+  static constexpr int QF = (8 * NF + THREADS - 1) / THREADS;  // face points per thread
+  static_assert(NF % 4 == 0, "face points in whole k-steps");
+};
+
+// per-element data of a staged group
+struct LsElem {
+  int64_t ub, fb;   // value offsets of the element in the state and face arrays
+  double geo[9];    // rx .. tz (constant over a straight-sided element)
+  double eps;
+  int ok, act;      // listed element; row in the active list (-1: not active)
+};
+
+template <int N>
+__device__ __forceinline__ void ls_stage_elems(const LsArgs &A, const int32_t *list, int n, int gi, LsElem *se,
+                                               bool with_geo) {
+  using C = LsCfg<N>;
+  constexpr int NP = C::NP, NF = C::NF;
+  const int t = threadIdx.x;
+  if (t < 8) {
+    LsElem x{};
+    x.act = -1;
+    if (8 * gi + t < n) {
+      const int64_t slot = list[8 * gi + t];
+      const int p = part_of_slot(A, slot);
+      const int64_t le = slot - A.slot_prefix[p];
+      x.ub = A.uoff[p] + le * NP;
+      x.fb = A.foff[p] + le * NF;
+      const int64_t gb = A.goff[p] + le * NP;
+      if (with_geo)
+        for (int m = 0; m < 9; ++m) x.geo[m] = A.geo[m][gb];
+      x.eps = A.eps[slot];
+      x.act = A.aslot[slot];
+      x.ok = 1;
     }
-    __syncwarp();
-    const double eps = A.eps[slot];
-    for (int i = lane; i < NP; i += 32) {
-      double ur = 0.0, us = 0.0, ut = 0.0;
-#pragma unroll 5
-      for (int j = 0; j < NP; ++j) {
-        const double v = su[j];
-        ur = fma(__ldg(A.Dr + j * NP + i), v, ur);
-        us = fma(__ldg(A.Ds + j * NP + i), v, us);
-        ut = fma(__ldg(A.Dt + j * NP + i), v, ut);
-      }
-      double q[3];
-      for (int d = 0; d < 3; ++d) q[d] = A.geo[d][gb + i] * ur + A.geo[3 + d][gb + i] * us + A.geo[6 + d][gb + i] * ut;
-#pragma unroll 6
-      for (int m = 0; m < NF; ++m) {
-        const double l = __ldg(A.LIFT + m * NP + i);
-        q[0] = fma(l, s_j[w][0][m], q[0]);
-        q[1] = fma(l, s_j[w][1][m], q[1]);
-        q[2] = fma(l, s_j[w][2][m], q[2]);
-      }
-      for (int d = 0; d < 3; ++d) A.eq[((int64_t)a * 3 + d) * NP + i] = eps * q[d];
-    }
-    __syncwarp();
+    se[t] = x;
   }
 }
 
 template <int N>
-__global__ void __launch_bounds__(32 * kLsWarps) ls_div_kernel(const LsArgs A) {
-  using O = Order<N>;
-  constexpr int NP = O::NP, NF = O::NF;
-  __shared__ double s_q[kLsWarps][3][NP], s_f[kLsWarps][NF];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int n = *reinterpret_cast<volatile const int *>(&A.counts[1]);
-  for (int r = blockIdx.x * kLsWarps + w; r < n; r += gridDim.x * kLsWarps) {
-    const int64_t slot = A.tlist[r];
-    const int p = part_of_slot(A, slot);
-    const int64_t le = slot - A.slot_prefix[p];
-    const int64_t gb = A.goff[p] + le * NP, fb = A.foff[p] + le * NF;
-    const int a = A.aslot[slot];
-    for (int i = lane; i < NP; i += 32)
-      for (int d = 0; d < 3; ++d) s_q[w][d][i] = a >= 0 ? A.eq[((int64_t)a * 3 + d) * NP + i] : 0.0;
-    __syncwarp();
-    for (int m = lane; m < NF; m += 32) {
-      const int32_t g = A.gmap[fb + m];
-      const int jM = A.fmask[m];
-      double ePq[3] = {0.0, 0.0, 0.0};
-      int node;
-      const int64_t ns = ((uint64_t)(int64_t)g < (uint64_t)A.n_u_values) ? slot_of_value(A, g, NP, &node) : -1;
-      if (ns >= 0) {
-        const int an = A.aslot[ns];
-        if (an >= 0)
-          for (int d = 0; d < 3; ++d) ePq[d] = A.eq[((int64_t)an * 3 + d) * NP + node];
-      } else {
-        atomicExch(A.status, kStatusBadGather);
-      }
-      double v = 0.0;
-      for (int d = 0; d < 3; ++d) v += A.face[d][fb + m] * (ePq[d] - s_q[w][d][jM]);
-      s_f[w][m] = 0.5 * A.face[3][fb + m] * v;
+__global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_grad_kernel(const LsArgs A) {
+  using C = LsCfg<N>;
+  constexpr int NP = C::NP, NF = C::NF, KT = C::KT, KL = C::KL, NPU = C::NPU, QF = C::QF;
+  __shared__ double su[8 * NPU], sj[3 * 8 * NF];
+  __shared__ LsElem se[8];
+  const int tid = threadIdx.x, lane = tid & 31, mt = tid >> 5;
+  const int ar = lane >> 2, ac = lane & 3, r = 8 * mt + ar;
+  const int n = *reinterpret_cast<volatile const int *>(&A.counts[0]);
+  const int ngroups = (n + 7) / 8;
+  for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
+    ls_stage_elems<N>(A, A.alist, n, gi, se, true);
+    __syncthreads();
+    for (int x = tid; x < 8 * NPU; x += C::THREADS) {
+      const int e = x / NPU, i = x - e * NPU;
+      su[x] = (se[e].ok && i < NP) ? (double)A.uhi[se[e].ub + i] + (double)A.ulo[se[e].ub + i] : 0.0;
     }
-    __syncwarp();
-    for (int i = lane; i < NP; i += 32) {
-      double div = 0.0;
-      if (a >= 0) {
-        double qr[3] = {0.0, 0.0, 0.0}, qs[3] = {0.0, 0.0, 0.0}, qt[3] = {0.0, 0.0, 0.0};
-#pragma unroll 5
-        for (int j = 0; j < NP; ++j) {
-          const double dr = __ldg(A.Dr + j * NP + i), ds = __ldg(A.Ds + j * NP + i), dt = __ldg(A.Dt + j * NP + i);
+    // this thread's face points: gather indices and face data, then the neighbour traces
+    int32_t g[QF];
+    double nd[QF][4];
+    bool use[QF];
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const double v = s_q[w][d][j];
-            qr[d] = fma(dr, v, qr[d]);
-            qs[d] = fma(ds, v, qs[d]);
-            qt[d] = fma(dt, v, qt[d]);
-          }
-        }
-        for (int d = 0; d < 3; ++d)
-          div += A.geo[d][gb + i] * qr[d] + A.geo[3 + d][gb + i] * qs[d] + A.geo[6 + d][gb + i] * qt[d];
-      }
-      double lift = 0.0;
-#pragma unroll 6
-      for (int m = 0; m < NF; ++m) lift = fma(__ldg(A.LIFT + m * NP + i), s_f[w][m], lift);
-      A.visc[(int64_t)r * NP + i] = div + lift;
+    for (int b = 0; b < QF; ++b) {
+      const int x = tid + C::THREADS * b, e = min(x / NF, 7), m = x - e * NF;
+      use[b] = x < 8 * NF && se[e].ok;
+      g[b] = use[b] ? A.gmap[se[e].fb + m] : 0;
+      for (int d = 0; d < 4; ++d) nd[b][d] = use[b] ? A.face[d][se[e].fb + m] : 0.0;
     }
-    __syncwarp();
+    float ph[QF], pl[QF];
+#pragma unroll
+    for (int b = 0; b < QF; ++b) {
+      const bool in = use[b] && (uint64_t)(int64_t)g[b] < (uint64_t)A.n_u_values;
+      if (use[b] && !in) {
+        atomicExch(A.status, kStatusBadGather);
+        g[b] = -1;  // rejected index: the interior trace stands
+      }
+      ph[b] = in ? A.uhi[g[b]] : 0.f;
+      pl[b] = in ? A.ulo[g[b]] : 0.f;
+    }
+    __syncthreads();  // su complete
+#pragma unroll
+    for (int b = 0; b < QF; ++b) {
+      const int x = tid + C::THREADS * b;
+      if (x < 8 * NF) {
+        const int e = x / NF, m = x - e * NF;
+        double jump = 0.0;
+        if (use[b]) {
+          const double uM = su[e * NPU + A.fmask[m]];
+          const double uP = g[b] < 0 ? uM : (double)ph[b] + (double)pl[b];
+          jump = 0.5 * (uP - uM) * nd[b][3];
+        }
+        for (int d = 0; d < 3; ++d) sj[(d * 8 + e) * NF + m] = nd[b][d] * jump;
+      }
+    }
+    __syncthreads();  // sj complete
+    double cr[2] = {0.0, 0.0}, cs[2] = {0.0, 0.0}, ct[2] = {0.0, 0.0};
+    double cl[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}};
+#pragma unroll
+    for (int kk = 0; kk < KT; ++kk) {
+      const int j = 4 * kk + ac;
+      const bool in = r < NP && j < NP;
+      const double bv = su[ar * NPU + j];
+      ls_dmma(cr[0], cr[1], in ? __ldg(A.Dr + j * NP + r) : 0.0, bv);
+      ls_dmma(cs[0], cs[1], in ? __ldg(A.Ds + j * NP + r) : 0.0, bv);
+      ls_dmma(ct[0], ct[1], in ? __ldg(A.Dt + j * NP + r) : 0.0, bv);
+    }
+#pragma unroll 5
+    for (int kk = 0; kk < KL; ++kk) {
+      const int m = 4 * kk + ac;
+      const double al = r < NP ? __ldg(A.LIFT + m * NP + r) : 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) ls_dmma(cl[d][0], cl[d][1], al, sj[(d * 8 + ar) * NF + m]);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int e = 2 * ac + h;
+      if (r < NP && se[e].ok) {
+        const LsElem &x = se[e];
+        for (int d = 0; d < 3; ++d) {
+          const double q = x.geo[d] * cr[h] + x.geo[3 + d] * cs[h] + x.geo[6 + d] * ct[h] + cl[d][h];
+          A.eq[((int64_t)(8 * gi + e) * 3 + d) * NP + r] = x.eps * q;
+        }
+      }
+    }
+    __syncthreads();  // the staging buffers are free for the next group
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_div_kernel(const LsArgs A) {
+  using C = LsCfg<N>;
+  constexpr int NP = C::NP, NF = C::NF, KT = C::KT, KL = C::KL, NPU = C::NPU, QF = C::QF;
+  __shared__ double sq[3 * 8 * NPU], sf[8 * NF];
+  __shared__ LsElem se[8];
+  const int tid = threadIdx.x, lane = tid & 31, mt = tid >> 5;
+  const int ar = lane >> 2, ac = lane & 3, r = 8 * mt + ar;
+  const int n = *reinterpret_cast<volatile const int *>(&A.counts[1]);
+  const int ngroups = (n + 7) / 8;
+  for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x) {
+    ls_stage_elems<N>(A, A.tlist, n, gi, se, true);
+    __syncthreads();
+    // the group's eps q_d, and this thread's face points: gather indices and face data
+    for (int x = tid; x < 3 * 8 * NPU; x += C::THREADS) {
+      const int d = x / (8 * NPU), y = x - d * 8 * NPU, e = y / NPU, i = y - e * NPU;
+      const int ae = se[e].act;
+      sq[x] = (ae >= 0 && i < NP) ? A.eq[((int64_t)ae * 3 + d) * NP + i] : 0.0;
+    }
+    int32_t g[QF];
+    double nd[QF][4];
+    bool use[QF];
+#pragma unroll
+    for (int b = 0; b < QF; ++b) {
+      const int x = tid + C::THREADS * b, e = min(x / NF, 7), m = x - e * NF;
+      use[b] = x < 8 * NF && se[e].ok;
+      g[b] = use[b] ? A.gmap[se[e].fb + m] : 0;
+      for (int d = 0; d < 4; ++d) nd[b][d] = use[b] ? A.face[d][se[e].fb + m] : 0.0;
+    }
+    // the neighbours' rows in the active list, then their eps q
+    int an[QF], node[QF];
+#pragma unroll
+    for (int b = 0; b < QF; ++b) {
+      an[b] = -1;
+      node[b] = 0;
+      if (use[b]) {
+        const int64_t ns =
+            ((uint64_t)(int64_t)g[b] < (uint64_t)A.n_u_values) ? slot_of_value(A, g[b], NP, &node[b]) : -1;
+        if (ns >= 0)
+          an[b] = A.aslot[ns];
+        else
+          atomicExch(A.status, kStatusBadGather);
+      }
+    }
+    double ePq[QF][3];
+#pragma unroll
+    for (int b = 0; b < QF; ++b)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) ePq[b][d] = an[b] >= 0 ? A.eq[((int64_t)an[b] * 3 + d) * NP + node[b]] : 0.0;
+    __syncthreads();  // sq complete
+#pragma unroll
+    for (int b = 0; b < QF; ++b) {
+      const int x = tid + C::THREADS * b;
+      if (x < 8 * NF) {
+        const int e = x / NF, m = x - e * NF;
+        double flux = 0.0;
+        if (use[b]) {
+          const int jM = A.fmask[m];
+          double v = 0.0;
+          for (int d = 0; d < 3; ++d) v += nd[b][d] * (ePq[b][d] - sq[(d * 8 + e) * NPU + jM]);
+          flux = 0.5 * nd[b][3] * v;
+        }
+        sf[e * NF + m] = flux;
+      }
+    }
+    __syncthreads();  // every surface flux formed from sq
+    // div(eps q) = sum_k D_k a_k with a_k = sum_d (d xi_k / d x_d) eps q_d (metrics constant over the element);
+    // a_k replaces eps q_d in place, each thread owning whole nodes
+    bool any_active = false;
+    for (int e = 0; e < 8; ++e) any_active |= se[e].act >= 0;
+    if (any_active) {
+      for (int y = tid; y < 8 * NPU; y += C::THREADS) {
+        const int e = y / NPU;
+        if (se[e].act >= 0) {
+          const double q0 = sq[y], q1 = sq[8 * NPU + y], q2 = sq[16 * NPU + y];
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+            sq[k * 8 * NPU + y] = se[e].geo[3 * k] * q0 + se[e].geo[3 * k + 1] * q1 + se[e].geo[3 * k + 2] * q2;
+        }
+      }
+      __syncthreads();
+    }
+    double c[3][2] = {{0.0, 0.0}, {0.0, 0.0}, {0.0, 0.0}}, cl[2] = {0.0, 0.0};
+    if (any_active) {
+#pragma unroll
+      for (int kk = 0; kk < KT; ++kk) {
+        const int j = 4 * kk + ac;
+        const bool in = r < NP && j < NP;
+        ls_dmma(c[0][0], c[0][1], in ? __ldg(A.Dr + j * NP + r) : 0.0, sq[ar * NPU + j]);
+        ls_dmma(c[1][0], c[1][1], in ? __ldg(A.Ds + j * NP + r) : 0.0, sq[(8 + ar) * NPU + j]);
+        ls_dmma(c[2][0], c[2][1], in ? __ldg(A.Dt + j * NP + r) : 0.0, sq[(16 + ar) * NPU + j]);
+      }
+    }
+#pragma unroll 5
+    for (int kk = 0; kk < KL; ++kk) {
+      const int m = 4 * kk + ac;
+      ls_dmma(cl[0], cl[1], r < NP ? __ldg(A.LIFT + m * NP + r) : 0.0, sf[ar * NF + m]);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int e = 2 * ac + h;
+      if (r < NP && se[e].ok) A.visc[(int64_t)(8 * gi + e) * NP + r] = (c[0][h] + c[1][h] + c[2][h]) + cl[h];
+    }
+    __syncthreads();  // the staging buffers are free for the next group
   }
 }
 
@@ -346,9 +535,9 @@ void launch_ls_n(const LsArgs &A, int num_sms, cudaStream_t st) {
   cuda_check(cudaGetLastError(), "ls_touch_kernel launch");
   ls_compact_kernel<<<num_sms * 4, 256, 0, st>>>(A);
   cuda_check(cudaGetLastError(), "ls_compact_kernel launch");
-  ls_grad_kernel<N><<<num_sms * 8, 32 * kLsWarps, 0, st>>>(A);
+  ls_grad_kernel<N><<<num_sms * 8, LsCfg<N>::THREADS, 0, st>>>(A);
   cuda_check(cudaGetLastError(), "ls_grad_kernel launch");
-  ls_div_kernel<N><<<num_sms * 8, 32 * kLsWarps, 0, st>>>(A);
+  ls_div_kernel<N><<<num_sms * 8, LsCfg<N>::THREADS, 0, st>>>(A);
   cuda_check(cudaGetLastError(), "ls_div_kernel launch");
 }
 

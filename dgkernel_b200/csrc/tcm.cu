@@ -416,6 +416,9 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       if (t + G < A.ntiles) tl_next = A.tiles[t + G];  // the next descriptor's load overlaps this tile
       const int ne = tl.nelem;
       const bool valid = e < ne;
+      // the learned-sensor viscosity: this element's row of viscous right-hand side, if it has one (the load
+      // is issued here so that its latency is spent before the epilogue)
+      const int vrow = (A.vslot && valid) ? A.vslot[tl.elem_slot + e] : -1;
       const bool got = mbar_wait_bounded(&full[s], (uint32_t)(k >> 1) & 1u, kSpinLimit) &&
                        mbar_wait_bounded(&hful[s], (uint32_t)(k >> 1) & 1u, kSpinLimit);
       unsigned char *slot = ring + (size_t)s * C::SLOT_B;
@@ -512,6 +515,17 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
         break;
       }
 
+      // the viscous right-hand side of this thread's nodes, loaded while the MMAs run
+      constexpr int NCE = ((NP + 7) / 8 + TPE - 1) / TPE;  // epilogue chunks per thread
+      float vv[NCE][8];
+#pragma unroll
+      for (int cc = 0; cc < NCE; ++cc)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int i = 8 * (h + TPE * cc) + q;
+          vv[cc][q] = (vrow >= 0 && i < NP) ? (float)A.visc[(int64_t)vrow * NP + i] : 0.f;
+        }
+
       // ---- volume epilogue while the LIFT MMAs run: t0 = a resu + dt vol for this thread's nodes ----
       const bool vdone = mbar_wait_bounded(mvol, (uint32_t)k & 1u, kSpinLimit);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -519,7 +533,6 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
         failed = true;
         break;
       }
-      constexpr int NCE = ((NP + 7) / 8 + TPE - 1) / TPE;  // epilogue chunks per thread
       float t0[NCE][8];
 #pragma unroll
       for (int cc = 0; cc < NCE; ++cc) {
@@ -541,8 +554,6 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
       const bool ldone = mbar_wait_bounded(mlift, (uint32_t)k & 1u, kSpinLimit);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t tail0 = ((uint32_t)(ne * NP * 4) & ~15u) / 4;  // nodes past the last full 16 B: plain stores
-      // the learned-sensor viscosity: this element's row of viscous right-hand side, if it has one
-      const int vrow = (A.vslot && valid) ? A.vslot[tl.elem_slot + e] : -1;
       if (ldone) {
 #pragma unroll
         for (int cc = 0; cc < NCE; ++cc) {
@@ -556,7 +567,7 @@ __global__ void __launch_bounds__(32 * (CW + 2), 1) rhs_stage_tcm_kernel(const M
               if (i < NP && valid) {
                 const int o = e * NP + i;
                 float rn = fmaf(dt, lf[q], t0[cc][q]);
-                if (vrow >= 0) rn = fmaf(dt, (float)A.visc[(int64_t)vrow * NP + i], rn);
+                if (vrow >= 0) rn = fmaf(dt, vv[cc][q], rn);
                 float hn, ln;
                 stage_update(hi[i], lo[i], rn, bh, bl, hn, ln);
                 sHi[o] = hn;
