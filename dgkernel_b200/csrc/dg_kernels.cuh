@@ -198,7 +198,7 @@ struct LsArgs {
   int32_t *aslot;              // per element slot: index in the active list or -1
   int32_t *alist, *tflag, *vslot, *tlist;
   int32_t *counts;             // [0] active, [1] touched, [2] network fallbacks to PP
-  double *eq;                  // [active][3][Np]: eps q
+  double *eq;                  // [active][Np][3]: eps q (a node's three components adjacent)
   double *visc;                // [touched][Np]: the viscous right-hand side
   int64_t nslots;
   int *status;

@@ -64,7 +64,7 @@ __device__ __forceinline__ int64_t slot_of_value(const LsArgs &A, int64_t g, int
 }
 
 template <int N>
-__global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A) {
+__global__ void __launch_bounds__(4 * kLsElems, 3) ls_sensor_kernel(const LsArgs A) {
   using O = Order<N>;
   constexpr int NP = O::NP;
   constexpr int NPP = NP + 1;  // padded row of the feature buffer
@@ -83,40 +83,45 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
   __syncthreads();
   const __half *W1 = sW, *b1 = W1 + kLsHid * NP, *W2 = b1 + kLsHid, *b2 = W2 + kLsHid * kLsHid, *w3 = b2 + kLsHid,
                *b3 = w3 + kLsHid;
-  // the state of the block's next 64 elements is loaded into registers while the current ones are computed
-  constexpr int FILL = (kLsElems * NP + 4 * kLsElems - 1) / (4 * kLsElems);  // values per thread
+  // Every warp walks its own groups of 8 elements (16 per 128-element tile) in rows 8 w .. 8 w + 7 of the
+  // block's buffers, with no block barrier; the state of its next group is loaded into registers while the
+  // current one is computed.
+  const int lane = tid & 31, w0 = (tid >> 5) * 8, nw = blockDim.x >> 5;
+  const int ngroups = 16 * A.ntiles;
+  constexpr int FILL = (8 * NP + 31) / 32;  // values per lane
   float fh[FILL], fl[FILL];
-  auto load = [&](int st) {
-    const MTile tl = A.tiles[st >> 1];
-    const int e0 = (st & 1) * kLsElems;  // half of the 128-element tile
-    const int ne = max(0, min(kLsElems, tl.nelem - e0));
+  auto load = [&](int gi) {
+    const MTile tl = A.tiles[gi >> 4];
+    const int e0 = (gi & 15) * 8;
+    const int ne = max(0, min(8, tl.nelem - e0));
     const int64_t base = tl.node_base + (int64_t)e0 * NP;
 #pragma unroll
     for (int q = 0; q < FILL; ++q) {
-      const int x = tid + q * 4 * kLsElems;
+      const int x = lane + 32 * q;
       fh[q] = x < ne * NP ? A.uhi[base + x] : 0.f;
       fl[q] = x < ne * NP ? A.ulo[base + x] : 0.f;
     }
   };
-  if ((int)blockIdx.x < 2 * A.ntiles) load(blockIdx.x);
-  for (int st = blockIdx.x; st < 2 * A.ntiles; st += gridDim.x) {
-    const MTile tl = A.tiles[st >> 1];
-    const int e0 = (st & 1) * kLsElems;  // half of the 128-element tile
-    const int ne = max(0, min(kLsElems, tl.nelem - e0));
+  const int g0 = blockIdx.x * nw + (tid >> 5), gstep = gridDim.x * nw;
+  if (g0 < ngroups) load(g0);
+  for (int gi = g0; gi < ngroups; gi += gstep) {
+    const MTile tl = A.tiles[gi >> 4];
+    const int e0 = (gi & 15) * 8;
+    const int ne = max(0, min(8, tl.nelem - e0));
 #pragma unroll
     for (int q = 0; q < FILL; ++q) {
-      const int x = tid + q * 4 * kLsElems;
-      if (x < kLsElems * NP) su[x] = (double)fh[q] + (double)fl[q];
+      const int x = lane + 32 * q;
+      if (x < 8 * NP) su[w0 * NP + x] = (double)fh[q] + (double)fl[q];
     }
-    __syncthreads();
-    if (st + (int)gridDim.x < 2 * A.ntiles) load(st + gridDim.x);
-    const bool valid = e < ne;
+    __syncwarp();
+    if (gi + gstep < ngroups) load(gi + gstep);
+    if (ne == 0) continue;  // past the tile's last element (warp-uniform)
+    const bool valid = (e & 7) < ne;
     // modal coefficients uhat = Vinv u of this warp's 8 elements on the FP64 tensor path (mma.sync m8n8k4):
     // A = Vinv (8-row m-tiles, 4-column k-steps), B = the elements' nodal values (one element per column);
     // they overwrite the warp's own rows of su
     {
       constexpr int MT = (NP + 7) / 8, KT = (NP + 3) / 4;
-      const int lane = tid & 31, w0 = (tid >> 5) * 8;
       const int ar = lane >> 2, ac = lane & 3, be = w0 + (lane >> 2);
       double c[MT][2];
 #pragma unroll
@@ -124,7 +129,7 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
 #pragma unroll
       for (int kk = 0; kk < KT; ++kk) {
         const int j = 4 * kk + ac;
-        const double bv = (j < NP && be < ne) ? su[be * NP + j] : 0.0;
+        const double bv = (j < NP && ar < ne) ? su[be * NP + j] : 0.0;
 #pragma unroll
         for (int mt = 0; mt < MT; ++mt) {
           const int r = 8 * mt + ar;
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
       }
       __syncwarp();
     }
-    const double *ue = su + (valid ? e : 0) * NP;  // now the element's modal coefficients
+    const double *ue = su + (valid ? e : w0) * NP;  // now the element's modal coefficients
     double tot = 0.0, top = 0.0;
     double uh[(NP + 3) / 4];
 #pragma unroll
@@ -209,7 +214,7 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
       }
     }
     if (valid && t == 0) {
-      const int64_t slot = tl.elem_slot + e0 + e;
+      const int64_t slot = tl.elem_slot + e0 + (e & 7);
       const double eps = A.eps0 * sig * A.h_over_n[slot];
       A.eps[slot] = eps;
       int a = -1;
@@ -220,7 +225,7 @@ __global__ void __launch_bounds__(4 * kLsElems) ls_sensor_kernel(const LsArgs A)
       A.aslot[slot] = a;
       if (fallback) atomicAdd(&A.counts[2], 1);
     }
-    __syncthreads();
+    __syncwarp();  // the warp's rows are free for its next group
   }
 }
 
@@ -390,7 +395,7 @@ __global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_grad_kernel(const LsArgs
         const LsElem &x = se[e];
         for (int d = 0; d < 3; ++d) {
           const double q = x.geo[d] * cr[h] + x.geo[3 + d] * cs[h] + x.geo[6 + d] * ct[h] + cl[d][h];
-          A.eq[((int64_t)(8 * gi + e) * 3 + d) * NP + r] = x.eps * q;
+          A.eq[((int64_t)(8 * gi + e) * NP + r) * 3 + d] = x.eps * q;
         }
       }
     }
@@ -412,10 +417,10 @@ __global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_div_kernel(const LsArgs 
     ls_stage_elems<N>(A, A.tlist, n, gi, se, true);
     __syncthreads();
     // the group's eps q_d, and this thread's face points: gather indices and face data
-    for (int x = tid; x < 3 * 8 * NPU; x += C::THREADS) {
-      const int d = x / (8 * NPU), y = x - d * 8 * NPU, e = y / NPU, i = y - e * NPU;
+    for (int x = tid; x < 3 * 8 * NPU; x += C::THREADS) {  // node-major reads: a node's 3 values are adjacent
+      const int e = x / (3 * NPU), y = x - e * 3 * NPU, i = y / 3, d = y - 3 * i;
       const int ae = se[e].act;
-      sq[x] = (ae >= 0 && i < NP) ? A.eq[((int64_t)ae * 3 + d) * NP + i] : 0.0;
+      sq[(d * 8 + e) * NPU + i] = (ae >= 0 && i < NP) ? A.eq[((int64_t)ae * NP + i) * 3 + d] : 0.0;
     }
     int32_t g[QF];
     double nd[QF][4];
@@ -446,7 +451,7 @@ __global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_div_kernel(const LsArgs 
 #pragma unroll
     for (int b = 0; b < QF; ++b)
 #pragma unroll
-      for (int d = 0; d < 3; ++d) ePq[b][d] = an[b] >= 0 ? A.eq[((int64_t)an[b] * 3 + d) * NP + node[b]] : 0.0;
+      for (int d = 0; d < 3; ++d) ePq[b][d] = an[b] >= 0 ? A.eq[((int64_t)an[b] * NP + node[b]) * 3 + d] : 0.0;
     __syncthreads();  // sq complete
 #pragma unroll
     for (int b = 0; b < QF; ++b) {
