@@ -344,7 +344,7 @@ struct DmmaCfg {
   static constexpr uint32_t STAGE_B = 11 * NODE_B + 4 * FACE_B;  // u, resu, 9 metrics, 4 face arrays
   static constexpr uint32_t GBUF_B = TE * NF * sizeof(T);         // gathered uP of one tile
   static constexpr uint32_t WORK_B = 2 * GBUF_B + TE * NFS * sizeof(T) + NF * sizeof(int32_t);
-  static constexpr size_t SMEM = 2 * (size_t)STAGE_B + WORK_B + 6 * sizeof(uint64_t);
+  static constexpr size_t SMEM = 2 * (size_t)STAGE_B + WORK_B + 8 * sizeof(uint64_t);
   static constexpr int MINB = 2 * SMEM <= 227 * 1024 ? 2 : 1;  // co-resident CTAs the launch bounds plan for
   static constexpr int GJ = (TE * NF + 31) / 32;                  // gathers per producer lane and tile
   static_assert(NODE_B % 16 == 0 && FACE_B % 16 == 0 && GBUF_B % 16 == 0, "smem slots must stay 16-byte aligned");
@@ -377,19 +377,28 @@ __device__ __forceinline__ bool cons_sync_and(bool p) {
   return r != 0;
 }
 
+// A tile's stage is filled in two parts with their own barriers: part A (the 9 metrics and 4 face arrays, read
+// by the volume products and the flux) and part B (u and resu, read until the update).
 template <int N>
-__device__ __forceinline__ void issue_tile_d(const RhsArgs<double> &A, const Tile &tl, char *stage, uint64_t *bar,
-                                             int rhs_only) {
+__device__ __forceinline__ void issue_tile_a(const RhsArgs<double> &A, const Tile &tl, char *stage, uint64_t *bar) {
   using C = DmmaCfg<N>;
   const uint32_t nb = round16((uint32_t)(tl.nelem * C::NP * sizeof(double)));
   const uint32_t fb = round16((uint32_t)(tl.nelem * C::NF * sizeof(double)));
-  mbar_expect_tx(bar, (rhs_only ? 10 : 11) * nb + 4 * fb);
-  bulk_g2s(stage, A.u_in + tl.node_base, nb, bar);
-  if (!rhs_only) bulk_g2s(stage + C::NODE_B, A.resu + tl.node_base, nb, bar);
+  mbar_expect_tx(bar, 9 * nb + 4 * fb);
 #pragma unroll
   for (int m = 0; m < 9; ++m) bulk_g2s(stage + (2 + m) * C::NODE_B, A.geo[m] + tl.node_base, nb, bar);
 #pragma unroll
   for (int m = 0; m < 4; ++m) bulk_g2s(stage + 11 * C::NODE_B + m * C::FACE_B, A.face[m] + tl.face_base, fb, bar);
+}
+
+template <int N>
+__device__ __forceinline__ void issue_tile_b(const RhsArgs<double> &A, const Tile &tl, char *stage, uint64_t *bar,
+                                             int rhs_only) {
+  using C = DmmaCfg<N>;
+  const uint32_t nb = round16((uint32_t)(tl.nelem * C::NP * sizeof(double)));
+  mbar_expect_tx(bar, (rhs_only ? 1 : 2) * nb);
+  bulk_g2s(stage, A.u_in + tl.node_base, nb, bar);
+  if (!rhs_only) bulk_g2s(stage + C::NODE_B, A.resu + tl.node_base, nb, bar);
 }
 
 // Warp-specialized CTA.  Producer warp: for tile k it reads the tile's gather map and the neighbour traces uP
@@ -411,12 +420,12 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
   T *gbuf = reinterpret_cast<T *>(ring + 2 * C::STAGE_B);  // [2][TE*NF] gathered uP
   T *sf = gbuf + 2 * TE * NF;                                // surface flux of the tile
   int *sfm = reinterpret_cast<int *>(sf + TE * NFS);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sfm + NF);    // full[2], gready[2], gfree[2]
-  uint64_t *full = bar, *gready = bar + 2, *gfree = bar + 4;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sfm + NF);    // fullA[2], gready[2], gfree[2], fullB[2]
+  uint64_t *full = bar, *gready = bar + 2, *gfree = bar + 4, *fullb = bar + 6;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = gridDim.x;
   if (tid == 0) {
-    for (int i = 0; i < 6; ++i) mbar_init(&bar[i], 1);
+    for (int i = 0; i < 8; ++i) mbar_init(&bar[i], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NF; i += C::THREADS) sfm[i] = A.fmask[i];
@@ -484,9 +493,12 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
 #pragma unroll
   for (int kk = 0; kk < KL; ++kk) aL[kk] = arow < NP ? A.LIFT[arow * LDL + 4 * kk + acol] : 0.0;
   if (tid == 0) {
-    if ((int)blockIdx.x < A.ntiles) issue_tile_d<N>(A, A.tiles[blockIdx.x], ring, &full[0], rhs_only);
-    if ((int)blockIdx.x + G < A.ntiles)
-      issue_tile_d<N>(A, A.tiles[blockIdx.x + G], ring + C::STAGE_B, &full[1], rhs_only);
+    for (int j = 0; j < 2; ++j)
+      if ((int)blockIdx.x + j * G < A.ntiles) {
+        const Tile tj = A.tiles[blockIdx.x + j * G];
+        issue_tile_a<N>(A, tj, ring + j * C::STAGE_B, &full[j]);
+        issue_tile_b<N>(A, tj, ring + j * C::STAGE_B, &fullb[j], rhs_only);
+      }
   }
   const T a = A.a, b = A.b, dt = A.dt;
   int k = 0;
@@ -494,11 +506,17 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
     const int s = k & 1;
     const uint32_t parity = (k >> 1) & 1;
     const bool ready = mbar_wait_bounded(&full[s], parity, kSpinLimit) &&
+                       mbar_wait_bounded(&fullb[s], parity, kSpinLimit) &&
                        mbar_wait_bounded(&gready[s], parity, kSpinLimit);
     if (!cons_sync_and<CONS>(ready)) {
       if (tid == 0) atomicExch(A.status, kStatusTimeoutCode);
+      // the copies in flight land before the CTA goes: this tile's and the next tile's
       mbar_wait_bounded(&full[s], parity, kSpinLimit);
-      if (t + G < A.ntiles) mbar_wait_bounded(&full[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
+      mbar_wait_bounded(&fullb[s], parity, kSpinLimit);
+      if (t + G < A.ntiles) {
+        mbar_wait_bounded(&full[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
+        mbar_wait_bounded(&fullb[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
+      }
       return;
     }
     const Tile tl = A.tiles[t];
@@ -557,7 +575,14 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
       }
     }
     cons_sync<CONS>();
-    if (tid == 0) mbar_arrive(&gfree[s]);  // the gathered traces of this tile are consumed
+    if (tid == 0) {
+      mbar_arrive(&gfree[s]);  // the gathered traces of this tile are consumed
+      // the metrics and face arrays of stage s are consumed too: tile t + 2G's part A streams in during (c)
+      if (t + 2 * G < A.ntiles) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        issue_tile_a<N>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &full[s]);
+      }
+    }
     // (c) LIFT * flux on the tensor path, LSERK4 update in the epilogue
     {
       T c[3][2];
@@ -585,10 +610,10 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
         }
       }
     }
-    cons_sync<CONS>();  // ring stage s and the flux buffer are free
+    cons_sync<CONS>();  // u and resu of stage s and the flux buffer are free
     if (tid == 0 && t + 2 * G < A.ntiles) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile_d<N>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &full[s], rhs_only);
+      issue_tile_b<N>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &fullb[s], rhs_only);
     }
   }
 }
