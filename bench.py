@@ -68,6 +68,14 @@ def b_alg_tcm(N: int, halo_per_elem: float) -> float:
     return 6 * 4 + (8 * 4 + 4 * 4 + 8 * halo_per_elem) / Np
 
 
+def b_alg_f64_compact(N: int) -> float:
+    """Algorithmic bytes per DOF-stage of the FP64 stage on the compact layout: u and resu read, u and resu
+    written (FP64), plus the per-element geometry (25 doubles) and compact connectivity (5 int32) spread over the
+    Np nodes."""
+    Np = (N + 1) * (N + 2) * (N + 3) // 6
+    return 4 * 8 + (25 * 8 + 5 * 4) / Np
+
+
 def kuhn_halo_per_elem(n: int, slabs: int, tile: int = 128) -> float:
     """Faces per element whose neighbour lies outside the element's tile (tiles of `tile` consecutive elements
     of one x-slab partition) on the periodic n^3 x 6 Kuhn mesh: the halo the tensor-core stage gathers."""
@@ -581,11 +589,13 @@ def run_burgers(args, world, rank, local):
     results = {}
     finals = {}
     # mixed_tc: the mixed stage with its element-local products on the tensor cores (orders 1..4)
-    forms = [("f64", np.float64, {}), ("f32", np.float32, {}), ("mixed", MIXED, {})]
+    # f64c: the FP64 stage on the compact layout (the control that separates layout from precision)
+    forms = [("f64", np.float64, {}), ("f64c", np.float64, {"compact": True}), ("f32", np.float32, {}),
+             ("mixed", MIXED, {})]
     if args.order <= 4:
         forms.append(("mixed_tc", MIXED, {"mma": True}))
-    kernels = {"f64": "rhs_stage_dmma_kernel", "f32": "rhs_stage_kernel", "mixed": "rhs_stage_mixed_kernel",
-               "mixed_tc": "rhs_stage_tcm_kernel"}
+    kernels = {"f64": "rhs_stage_dmma_kernel", "f64c": "rhs_stage_dmma_kernel (compact)", "f32": "rhs_stage_kernel",
+               "mixed": "rhs_stage_mixed_kernel", "mixed_tc": "rhs_stage_tcm_kernel"}
     micro = None
     for name, dt, kw in forms:
         if name == "f64":
@@ -602,6 +612,7 @@ def run_burgers(args, world, rank, local):
         results[name] = {"ms": ms, "dofs": prob.dofs, "clocks": clk.summary(), "prob": prob,
                          "b_alg": b_alg_tcm(args.order, kuhn_halo_per_elem(args.n, args.slabs))
                          if name == "mixed_tc" else b_alg_mixed(args.order) if name == "mixed" else
+                         b_alg_f64_compact(args.order) if name == "f64c" else
                          b_alg_per_dof(args.order, 8 if name == "f64" else 4),
                          "kernel": kernels[name]}
         if name != "f64":
@@ -624,7 +635,7 @@ def run_burgers(args, world, rank, local):
                               **dt_kw[1])
     r = prob.runner
     state = ("uhi", "ulo", "resu") if chosen.startswith("mixed") else ("u", "resu")
-    hdt = torch.float32 if chosen != "f64" else torch.float64
+    hdt = torch.float64 if chosen in ("f64", "f64c") else torch.float32
     hosts = {nm: torch.empty(dofs, dtype=hdt, pin_memory=True).numpy() for nm in state}
     for nm, h in hosts.items():
         r.CopyFromDevice(nm, h)
@@ -665,7 +676,7 @@ def run_burgers(args, world, rank, local):
         out = {
             "metric": METRIC, "value": thr[chosen], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ch["ms"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": {"f64": "f64", "f32": "f32", "mixed": "f32x2+f32",
+            "vs_baseline": None, "dtype": {"f64": "f64", "f64c": "f64", "f32": "f32", "mixed": "f32x2+f32",
                                                   "mixed_tc": "f32x2+f32 (bf16x3 products, f32 acc)"}[chosen],
             "data": "synthetic",
             "config": {"workload": f"3-D Burgers tet-DG, order {args.order} (Np={Np}), periodic {args.n}^3x6 Kuhn "
@@ -679,6 +690,9 @@ def run_burgers(args, world, rank, local):
                           "hbm_frac": results[k]["b_alg"] * dofs / (results[k]["ms"] * 1e-3) / 1e9 / hbm}
                       for k in thr},
             "chosen_vs_plain_fp64": {"speedup": thr[chosen] / thr["f64"], "l2_err": errs[chosen]},
+            # the same FP64 arithmetic on the compact layout: what the layout buys and what precision adds
+            "chosen_vs_compact_fp64": {"speedup": thr[chosen] / thr["f64c"], "compact_fp64_vs_plain_fp64":
+                                       thr["f64c"] / thr["f64"]} if "f64c" in thr else None,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                          "b_alg_per_dof": bpd, "kernel": ch["kernel"]},

@@ -218,6 +218,8 @@ class _TetBurgers:
         if self.visc:
             return f"rhsStageAV({self._av_args(self.visc)})"
         if not self.mixed:
+            if getattr(self, "compact", False):
+                return f"rhsStage(conservative={self.conservative},compact=1)"
             return f"rhsStage(conservative={self.conservative})"
         args = [f"conservative={self.conservative}"]
         if getattr(self, "tensor", None) is not None:
@@ -334,8 +336,11 @@ class BurgersProblem(_TetBurgers):
     def __init__(self, N: int, n: int, nslab: int = 1, dtype=np.float64, u0: str = "sine", seed: int = DEFAULT_SEED,
                  cfl: float = 0.3, conservative: int = 0, stream=None, u0_host=None, warps=None, ring=None,
                  viscosity=None, eps0: float = 1.0, c0: float = 0.0, kappa: float = 1.0, conf=(0.1, 0.9),
-                 mode_sigma: float = 0.1, tensor=None, mma=None, derivatives=False, learned=None):
+                 mode_sigma: float = 0.1, tensor=None, mma=None, derivatives=False, learned=None, compact=False):
         self.n, self.nslab = n, nslab
+        # float64 stage on the compact layout: per-element geometry and compact connectivity (straight-sided
+        # elements), the same FP64 tensor-path arithmetic as the plain stage
+        self.compact = compact
         # mixed tensor-core stage with learned-sensor (or PP) artificial viscosity: "pp", "mlp" or "mlp0"
         self.learned = learned
         self.derivatives = derivatives  # also bind DuDx, DuDy, DuDz for the `differentiate` operator

@@ -77,7 +77,17 @@ struct RhsArgs {
   T a, b, dt;            // LSERK stage coefficients
   int conservative;      // 0: -u (ux+uy+uz) (reference form), 1: -div(u^2/2 (1,1,1))
   int *status;
+  // compact FP64 form (straight-sided elements): kCompactGeo64 values per element slot, compact connectivity
+  // (kMixedConnWords per slot) with its face-order table, and each tile's first element slot
+  const double *geoc;
+  const int32_t *conn;
+  const uint8_t *ftab;
+  int ncodes;
+  const int64_t *tile_slot;
 };
+
+// compact FP64 geometry per element: rx .. tz, then per face nx, ny, nz, Fscale
+constexpr int kCompactGeo64 = 25;
 
 template <typename T>
 struct DiffArgs {

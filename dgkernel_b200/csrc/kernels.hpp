@@ -49,6 +49,9 @@ void prepare_rhs_tcm(int N, int consumer_warps);  // attributes, before any stre
 bool launch_rhs_tcm(int N, const MixedArgs &A, int consumer_warps, int num_sms, cudaStream_t st, LaunchInfo *info);
 template <typename T>
 void launch_compact_geometry(const CompactGeoArgs<T> &g, cudaStream_t st);
+// Compact FP64 geometry (kCompactGeo64 values per element slot) for the compact form of the FP64 stage;
+// g.out is unused, g.bad counts elements that are not straight-sided.
+void launch_compact_geo64(const CompactGeoArgs<double> &g, double *out, cudaStream_t st);
 void launch_split_join(const SplitJoinArgs &a, cudaStream_t st);
 
 // Precision form with exact integer products on the tensor cores (oz.cu): orders 4..7, tiles of

@@ -327,7 +327,9 @@ template <> struct DmmaShape<3> { static constexpr int TE = 8; };
 template <> struct DmmaShape<4> { static constexpr int TE = 8; };
 template <> struct DmmaShape<5> { static constexpr int TE = 8; };
 
-template <int N>
+// CP: compact FP64 form (per element: the kCompactGeo64 constant geometry values instead of the 9 metric and
+// 4 face arrays; neighbour traces through the compact connectivity instead of the gather map)
+template <int N, bool CP = false>
 struct DmmaCfg {
   using O = Order<N>;
   using T = double;
@@ -341,13 +343,18 @@ struct DmmaCfg {
   static constexpr int THREADS = CONS + 32;  // + one producer warp gathering neighbour traces
   static constexpr uint32_t NODE_B = TE * NP * sizeof(T);
   static constexpr uint32_t FACE_B = TE * NF * sizeof(T);
-  static constexpr uint32_t STAGE_B = 11 * NODE_B + 4 * FACE_B;  // u, resu, 9 metrics, 4 face arrays
+  static constexpr uint32_t GEOC_B = (uint32_t)TE * kCompactGeo64 * sizeof(T);
+  // u, resu, then 9 metrics and 4 face arrays, or the compact geometry
+  static constexpr uint32_t STAGE_B = CP ? 2 * NODE_B + GEOC_B : 11 * NODE_B + 4 * FACE_B;
   static constexpr uint32_t GBUF_B = TE * NF * sizeof(T);         // gathered uP of one tile
   static constexpr uint32_t WORK_B = 2 * GBUF_B + TE * NFS * sizeof(T) + NF * sizeof(int32_t);
-  static constexpr size_t SMEM = 2 * (size_t)STAGE_B + WORK_B + 8 * sizeof(uint64_t);
+  static constexpr int FTR = (NF / 4 + 15) & ~15;        // face-order table row: Nfp bytes rounded up to 16
+  static constexpr uint32_t FTAB_B = CP ? 256 * FTR : 0;
+  static constexpr size_t SMEM = 2 * (size_t)STAGE_B + WORK_B + 8 * sizeof(uint64_t) + FTAB_B;
   static constexpr int MINB = 2 * SMEM <= 227 * 1024 ? 2 : 1;  // co-resident CTAs the launch bounds plan for
   static constexpr int GJ = (TE * NF + 31) / 32;                  // gathers per producer lane and tile
-  static_assert(NODE_B % 16 == 0 && FACE_B % 16 == 0 && GBUF_B % 16 == 0, "smem slots must stay 16-byte aligned");
+  static_assert(NODE_B % 16 == 0 && FACE_B % 16 == 0 && GBUF_B % 16 == 0 && GEOC_B % 16 == 0,
+                "smem slots must stay 16-byte aligned");
   static_assert(TE % 8 == 0 && NF % 4 == 0, "tile must be whole n-tiles");
 };
 
@@ -379,9 +386,15 @@ __device__ __forceinline__ bool cons_sync_and(bool p) {
 
 // A tile's stage is filled in two parts with their own barriers: part A (the 9 metrics and 4 face arrays, read
 // by the volume products and the flux) and part B (u and resu, read until the update).
-template <int N>
-__device__ __forceinline__ void issue_tile_a(const RhsArgs<double> &A, const Tile &tl, char *stage, uint64_t *bar) {
-  using C = DmmaCfg<N>;
+template <int N, bool CP>
+__device__ __forceinline__ void issue_tile_a(const RhsArgs<double> &A, const Tile &tl, int64_t slot, char *stage,
+                                             uint64_t *bar) {
+  using C = DmmaCfg<N, CP>;
+  if (CP) {  // the compact geometry of the tile's element slots (slots are padded to whole tiles)
+    mbar_expect_tx(bar, C::GEOC_B);
+    bulk_g2s(stage + 2 * C::NODE_B, A.geoc + slot * kCompactGeo64, C::GEOC_B, bar);
+    return;
+  }
   const uint32_t nb = round16((uint32_t)(tl.nelem * C::NP * sizeof(double)));
   const uint32_t fb = round16((uint32_t)(tl.nelem * C::NF * sizeof(double)));
   mbar_expect_tx(bar, 9 * nb + 4 * fb);
@@ -391,10 +404,10 @@ __device__ __forceinline__ void issue_tile_a(const RhsArgs<double> &A, const Til
   for (int m = 0; m < 4; ++m) bulk_g2s(stage + 11 * C::NODE_B + m * C::FACE_B, A.face[m] + tl.face_base, fb, bar);
 }
 
-template <int N>
+template <int N, bool CP>
 __device__ __forceinline__ void issue_tile_b(const RhsArgs<double> &A, const Tile &tl, char *stage, uint64_t *bar,
                                              int rhs_only) {
-  using C = DmmaCfg<N>;
+  using C = DmmaCfg<N, CP>;
   const uint32_t nb = round16((uint32_t)(tl.nelem * C::NP * sizeof(double)));
   mbar_expect_tx(bar, (rhs_only ? 1 : 2) * nb);
   bulk_g2s(stage, A.u_in + tl.node_base, nb, bar);
@@ -407,9 +420,10 @@ __device__ __forceinline__ void issue_tile_b(const RhsArgs<double> &A, const Til
 // (a) [Dr;Ds;Dt] * U on the tensor path with the metrics applied in the epilogue (volume terms stay in
 // registers), (b) the Lax-Friedrichs flux of their face points, (c) LIFT * flux on the tensor path with the
 // LSERK4 update in the epilogue, streamed to HBM.  Two consumer barriers per tile.
-template <int N>
-__global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_stage_dmma_kernel(RhsArgs<double> A, int rhs_only) {
-  using C = DmmaCfg<N>;
+template <int N, bool CP>
+__global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
+    rhs_stage_dmma_kernel(RhsArgs<double> A, int rhs_only) {
+  using C = DmmaCfg<N, CP>;
   using T = double;
   constexpr int NP = C::NP, NF = C::NF, NFS = C::NFS, TE = C::TE, CONS = C::CONS;
   constexpr int KT = C::KT, KL = C::KL, MT = C::MT, GJ = C::GJ;
@@ -422,6 +436,7 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
   int *sfm = reinterpret_cast<int *>(sf + TE * NFS);
   uint64_t *bar = reinterpret_cast<uint64_t *>(sfm + NF);    // fullA[2], gready[2], gfree[2], fullB[2]
   uint64_t *full = bar, *gready = bar + 2, *gfree = bar + 4, *fullb = bar + 6;
+  uint8_t *sft = reinterpret_cast<uint8_t *>(bar + 8);  // compact form: face-order rows of C::FTR bytes
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = gridDim.x;
   if (tid == 0) {
@@ -429,6 +444,13 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NF; i += C::THREADS) sfm[i] = A.fmask[i];
+  if (CP) {
+    constexpr int NFP = NF / 4;
+    for (int i = tid; i < min(A.ncodes, 256) * C::FTR; i += C::THREADS) {
+      const int row = i / C::FTR, col = i - row * C::FTR;
+      sft[i] = col < NFP ? A.ftab[row * NFP + col] : 0;
+    }
+  }
   __syncthreads();
 
   if (tid >= CONS) {
@@ -443,10 +465,27 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
       const Tile tl = A.tiles[t];
       const int nfc = tl.nelem * NF;
       int32_t src[GJ];
+      if (CP) {  // neighbour base and face-order code of the point's face, then the point's node in it
+        constexpr int NFP = NF / 4;
+        const int64_t slot0 = A.tile_slot[t];
+        const int ncd = min(A.ncodes, 256);
 #pragma unroll
-      for (int j = 0; j < GJ; ++j) {
-        const int idx = lane + 32 * j;
-        src[j] = idx < nfc ? __ldcs(A.gmap + tl.face_base + idx) : 0;
+        for (int j = 0; j < GJ; ++j) {
+          const int idx = lane + 32 * j;
+          src[j] = 0;
+          if (idx < nfc) {
+            const int e = idx / NF, q = idx - e * NF, f = q / NFP, p = q - f * NFP;
+            const int32_t *cn = A.conn + (slot0 + e) * kMixedConnWords;
+            const int cd = min((int)(((uint32_t)cn[4] >> (8 * f)) & 0xffu), ncd - 1);
+            src[j] = cn[f] + sft[cd * C::FTR + p];
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < GJ; ++j) {
+          const int idx = lane + 32 * j;
+          src[j] = idx < nfc ? __ldcs(A.gmap + tl.face_base + idx) : 0;
+        }
       }
       T up[GJ];
 #pragma unroll
@@ -496,8 +535,8 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
     for (int j = 0; j < 2; ++j)
       if ((int)blockIdx.x + j * G < A.ntiles) {
         const Tile tj = A.tiles[blockIdx.x + j * G];
-        issue_tile_a<N>(A, tj, ring + j * C::STAGE_B, &full[j]);
-        issue_tile_b<N>(A, tj, ring + j * C::STAGE_B, &fullb[j], rhs_only);
+        issue_tile_a<N, CP>(A, tj, CP ? A.tile_slot[blockIdx.x + j * G] : 0, ring + j * C::STAGE_B, &full[j]);
+        issue_tile_b<N, CP>(A, tj, ring + j * C::STAGE_B, &fullb[j], rhs_only);
       }
   }
   const T a = A.a, b = A.b, dt = A.dt;
@@ -524,7 +563,7 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
     const char *stage = ring + s * C::STAGE_B;
     const T *su = reinterpret_cast<const T *>(stage);
     const T *sr = su + TE * NP;
-    const T *sg = sr + TE * NP;
+    const T *sg = sr + TE * NP;  // per-node metrics; in the compact form the per-element geometry
     const T *sfc = reinterpret_cast<const T *>(stage + 11 * C::NODE_B);
     const T *g = gbuf + s * TE * NF;
 
@@ -551,9 +590,12 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
         if (arow < NP && e < ne) {
           const int o = e * NP + arow;
           const T ur = c[0][0][h] + c[0][1][h], us = c[1][0][h] + c[1][1][h], ut = c[2][0][h] + c[2][1][h];
-          const T ux = sg[0 * TE * NP + o] * ur + sg[3 * TE * NP + o] * us + sg[6 * TE * NP + o] * ut;
-          const T uy = sg[1 * TE * NP + o] * ur + sg[4 * TE * NP + o] * us + sg[7 * TE * NP + o] * ut;
-          const T uz = sg[2 * TE * NP + o] * ur + sg[5 * TE * NP + o] * us + sg[8 * TE * NP + o] * ut;
+          T m9[9];
+#pragma unroll
+          for (int m = 0; m < 9; ++m) m9[m] = CP ? sg[e * kCompactGeo64 + m] : sg[m * TE * NP + o];
+          const T ux = m9[0] * ur + m9[3] * us + m9[6] * ut;
+          const T uy = m9[1] * ur + m9[4] * us + m9[7] * ut;
+          const T uz = m9[2] * ur + m9[5] * us + m9[8] * ut;
           vol[h] = A.conservative ? -(ux + uy + uz) : -su[o] * (ux + uy + uz);
         }
       }
@@ -566,12 +608,13 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
         const int e = idx / NF, q = idx - e * NF;
         const T uM = su[e * NP + sfm[q]];
         const T uP = g[idx];
-        const T nsum = sfc[idx] + sfc[TE * NF + idx] + sfc[2 * TE * NF + idx];
+        const T *gf = sg + e * kCompactGeo64 + 9 + 4 * (q / (NF / 4));  // compact form: the face's nx ny nz Fscale
+        const T nsum = CP ? gf[0] + gf[1] + gf[2] : sfc[idx] + sfc[TE * NF + idx] + sfc[2 * TE * NF + idx];
         const T fM = 0.5 * uM * uM * nsum, fP = 0.5 * uP * uP * nsum;
         const T an = fabs(nsum);
         const T lam = fmax(fabs(uM) * an, fabs(uP) * an);
         const T du = fM - (0.5 * (fM + fP) + 0.5 * lam * (uM - uP));
-        sf[e * NFS + q] = sfc[3 * TE * NF + idx] * du;
+        sf[e * NFS + q] = (CP ? gf[3] : sfc[3 * TE * NF + idx]) * du;
       }
     }
     cons_sync<CONS>();
@@ -580,7 +623,7 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
       // the metrics and face arrays of stage s are consumed too: tile t + 2G's part A streams in during (c)
       if (t + 2 * G < A.ntiles) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue_tile_a<N>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &full[s]);
+        issue_tile_a<N, CP>(A, A.tiles[t + 2 * G], CP ? A.tile_slot[t + 2 * G] : 0, ring + s * C::STAGE_B, &full[s]);
       }
     }
     // (c) LIFT * flux on the tensor path, LSERK4 update in the epilogue
@@ -613,16 +656,16 @@ __global__ void __launch_bounds__(DmmaCfg<N>::THREADS, DmmaCfg<N>::MINB) rhs_sta
     cons_sync<CONS>();  // u and resu of stage s and the flux buffer are free
     if (tid == 0 && t + 2 * G < A.ntiles) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile_b<N>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &fullb[s], rhs_only);
+      issue_tile_b<N, CP>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &fullb[s], rhs_only);
     }
   }
 }
 
-template <int N>
+template <int N, bool CP>
 static bool dmma_launch_n(const RhsArgs<double> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info) {
-  using C = DmmaCfg<N>;
+  using C = DmmaCfg<N, CP>;
   if (C::SMEM > 227 * 1024) return false;
-  auto k = rhs_stage_dmma_kernel<N>;
+  auto k = rhs_stage_dmma_kernel<N, CP>;
   cuda_check(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM), "smem attr");
   int per = 0;
   cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, C::THREADS, C::SMEM), "occupancy");
@@ -633,13 +676,60 @@ static bool dmma_launch_n(const RhsArgs<double> &A, int rhs_only, int num_sms, c
   return true;
 }
 
+// Compact FP64 geometry of the compact form: per element slot the node-0 metrics and, per face, the first face
+// point's nx, ny, nz and Fscale; an element whose values vary over its nodes or face points by more than 1e-6
+// of the row's scale (the mixed stage's rule: node-to-node round-off of the FP64 metrics, where a curved
+// element differs by O(h)) is counted in *bad (the form needs straight-sided elements).
+__global__ void compact_geo64_kernel(CompactGeoArgs<double> g, double *out) {
+  const int nfp = g.nf / 4;
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < g.elem_total;
+       x += (int64_t)gridDim.x * blockDim.x) {
+    int p = 0;
+    while (p + 1 < g.npart && g.elem_prefix[p + 1] <= x) ++p;
+    const int64_t le = x - g.elem_prefix[p];
+    const int64_t nb = g.node_off[p] + le * g.np, fb = g.face_off[p] + le * g.nf;
+    double *o = out + (g.slot_prefix[p] + le) * kCompactGeo64;
+    bool bad = false;
+    for (int d = 0; d < 3; ++d) {
+      double scale = 0.0;
+      for (int q = 0; q < 3; ++q) scale = fmax(scale, fabs(g.geo[3 * d + q][nb]));
+      for (int q = 0; q < 3; ++q) {
+        const int m = 3 * d + q;
+        const double v = g.geo[m][nb];
+        for (int i = 1; i < g.np; ++i) bad |= !(fabs(g.geo[m][nb + i] - v) <= 1e-6 * scale);
+        o[m] = v;
+      }
+    }
+    for (int f = 0; f < 4; ++f) {
+      const int64_t q0 = fb + f * nfp;
+      const double ns = fmax(fabs(g.face[0][q0]), fmax(fabs(g.face[1][q0]), fabs(g.face[2][q0])));
+      for (int c = 0; c < 4; ++c) {
+        const double v = g.face[c][q0], sc = c < 3 ? ns : fabs(v);
+        for (int q = 1; q < nfp; ++q) bad |= !(fabs(g.face[c][q0 + q] - v) <= 1e-6 * sc);
+        o[9 + 4 * f + c] = v;
+      }
+    }
+    if (bad) atomicAdd(g.bad, 1);
+  }
+}
+
+void launch_compact_geo64(const CompactGeoArgs<double> &g, double *out, cudaStream_t st) {
+  compact_geo64_kernel<<<592, 256, 0, st>>>(g, out);
+  cuda_check(cudaGetLastError(), "compact_geo64_kernel launch");
+}
+
 bool launch_rhs_dmma(int N, const RhsArgs<double> &A, int rhs_only, int num_sms, cudaStream_t st, LaunchInfo *info) {
   switch (N) {
-    case 1: return dmma_launch_n<1>(A, rhs_only, num_sms, st, info);
-    case 2: return dmma_launch_n<2>(A, rhs_only, num_sms, st, info);
-    case 3: return dmma_launch_n<3>(A, rhs_only, num_sms, st, info);
-    case 4: return dmma_launch_n<4>(A, rhs_only, num_sms, st, info);
-    case 5: return dmma_launch_n<5>(A, rhs_only, num_sms, st, info);
+    case 1: return A.geoc ? dmma_launch_n<1, true>(A, rhs_only, num_sms, st, info)
+                   : dmma_launch_n<1, false>(A, rhs_only, num_sms, st, info);
+    case 2: return A.geoc ? dmma_launch_n<2, true>(A, rhs_only, num_sms, st, info)
+                   : dmma_launch_n<2, false>(A, rhs_only, num_sms, st, info);
+    case 3: return A.geoc ? dmma_launch_n<3, true>(A, rhs_only, num_sms, st, info)
+                   : dmma_launch_n<3, false>(A, rhs_only, num_sms, st, info);
+    case 4: return A.geoc ? dmma_launch_n<4, true>(A, rhs_only, num_sms, st, info)
+                   : dmma_launch_n<4, false>(A, rhs_only, num_sms, st, info);
+    case 5: return A.geoc ? dmma_launch_n<5, true>(A, rhs_only, num_sms, st, info)
+                   : dmma_launch_n<5, false>(A, rhs_only, num_sms, st, info);
     default: return false;
   }
 }

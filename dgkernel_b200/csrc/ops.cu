@@ -215,11 +215,15 @@ struct RhsOp : Op {
   int N, ntiles, rhs_only, conservative;
   Binding *u, *unext = nullptr, *resu = nullptr, *rhs = nullptr, *geo[9], *face[4], *gmap;
   DevBuf dmat, lift, fmask, tiles;
+  // compact=1 (FP64): per-element geometry, compact connectivity and face-order table, each tile's first slot
+  int compact = 0, ncodes = 0;
+  DevBuf geoc, cconn, cftab, tslot;
   LaunchInfo info;
   RhsOp(Runner &r, Roles &R, int only) : rhs_only(only) {
     static const char *gn[9] = {"Rx", "Ry", "Rz", "Sx", "Sy", "Sz", "Tx", "Ty", "Tz"};
     static const char *fn[4] = {"nx", "ny", "nz", "Fscale"};
     conservative = R.flag("conservative", 0);
+    compact = R.flag("compact", 0);
     // halo=1: the last partition holds neighbour values received from other ranks (slab exchange); it is read
     // through the gather map and never advanced
     const int halo = R.flag("halo", 0);
@@ -281,8 +285,12 @@ struct RhsOp : Op {
         use_tma = true;
         ntiles = (int)tl.size();
         tiles.upload(tl.data(), tl.size() * sizeof(Tile));
+        if (compact) build_compact(r, R, tl, (int)np, nfp, tile_parts);
       }
     }
+    if (compact && !use_tma)
+      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": compact=1 is built for the FP64 tensor-path stage (orders 1..5, "
+                                                 "16-byte aligned partitions)");
     if (!use_tma) {
       auto tl = make_tiles(r, *u, face[0], tile_elems(N), (int)np, nf, tile_parts);
       ntiles = (int)tl.size();
@@ -290,6 +298,64 @@ struct RhsOp : Op {
     }
   }
   bool use_tma = false;
+  // The compact form's inputs, derived once from the bound arrays: the per-element geometry (checked
+  // straight-sided), the gather map as neighbour bases and face-order codes, and each tile's first slot.
+  void build_compact(Runner &r, Roles &R, const std::vector<Tile> &tl, int np, int nfp, int tile_parts) {
+    const int P = r.npart;
+    std::vector<int64_t> sp((size_t)P + 1, 0), ep((size_t)P + 1, 0);
+    for (int p = 0; p < P; ++p) {
+      sp[(size_t)p + 1] = sp[(size_t)p] + slot_padded(r.K[p]);
+      ep[(size_t)p + 1] = ep[(size_t)p] + r.K[p];
+    }
+    const int64_t nslots = std::max<int64_t>(sp[(size_t)P], 1);
+    {
+      std::vector<double> z((size_t)(nslots * kCompactGeo64), 0.0);
+      geoc.upload(z.data(), z.size() * sizeof(double));
+    }
+    DevBuf dep, dsp, dno, dfo, dbad;
+    dep.upload(ep.data(), sizeof(int64_t) * (P + 1));
+    dsp.upload(sp.data(), sizeof(int64_t) * P);
+    dno.upload(geo[0]->offsets.data(), sizeof(int64_t) * P);
+    dfo.upload(face[0]->offsets.data(), sizeof(int64_t) * P);
+    int zero = 0;
+    dbad.upload(&zero, sizeof(int));
+    CompactGeoArgs<double> g{};
+    g.npart = P;
+    g.np = np;
+    g.nf = 4 * nfp;
+    g.elem_total = ep[(size_t)P];
+    g.elem_prefix = dep.get<int64_t>();
+    g.slot_prefix = dsp.get<int64_t>();
+    g.node_off = dno.get<int64_t>();
+    g.face_off = dfo.get<int64_t>();
+    for (int i = 0; i < 9; ++i) g.geo[i] = reinterpret_cast<const double *>(geo[i]->dptr);
+    for (int i = 0; i < 4; ++i) g.face[i] = reinterpret_cast<const double *>(face[i]->dptr);
+    g.bad = dbad.get<int>();
+    launch_compact_geo64(g, geoc.get<double>(), r.stream());
+    int bad = 0;
+    cuda_check(cudaMemcpyAsync(&bad, dbad.p, sizeof(int), cudaMemcpyDeviceToHost, r.stream()), "read affinity check");
+    cuda_check(cudaStreamSynchronize(r.stream()), "compact geometry");
+    if (bad)
+      throw Error(DGK_ERR_UNSUPPORTED, R.kname + ": compact=1 needs straight-sided elements; " + std::to_string(bad) +
+                                           " elements have metrics or face factors that vary by more than 1e-6");
+    std::vector<int32_t> gm((size_t)gmap->offsets.back());
+    cuda_check(cudaMemcpy(gm.data(), gmap->dptr, gm.size() * sizeof(int32_t), cudaMemcpyDeviceToHost), "read gmap");
+    CompactFaces cf;
+    try {
+      cf = compact_faces(P, r.K.data(), u->offsets.data(), gmap->offsets.data(), sp.data(), np, nfp, gm.data());
+    } catch (const std::exception &ex) {
+      throw Error(DGK_ERR_INVALID, R.kname + ": " + ex.what());
+    }
+    ncodes = std::max(cf.ncodes, 1);
+    if (cf.table.empty()) cf.table.assign((size_t)nfp, 0);
+    cconn.upload(cf.conn.data(), std::max<size_t>(cf.conn.size(), 1) * sizeof(int32_t));
+    cftab.upload(cf.table.data(), cf.table.size());
+    std::vector<int64_t> ts(tl.size());
+    for (size_t i = 0; i < tl.size(); ++i)
+      ts[i] = sp[(size_t)tl[i].part] + (tl[i].node_base - u->offsets[(size_t)tl[i].part]) / np;
+    tslot.upload(ts.data(), std::max<size_t>(ts.size(), 1) * sizeof(int64_t));
+    (void)tile_parts;
+  }
   std::vector<std::string> scalar_names() const override {
     if (rhs_only) return {};
     return {"a", "b", "dt"};
@@ -316,6 +382,13 @@ struct RhsOp : Op {
     }
     A.conservative = conservative;
     A.status = r.status_word();
+    if (compact) {
+      A.geoc = geoc.get<double>();
+      A.conn = cconn.get<int32_t>();
+      A.ftab = cftab.get<uint8_t>();
+      A.ncodes = ncodes;
+      A.tile_slot = tslot.get<int64_t>();
+    }
     bool done = false;
     if constexpr (std::is_same<T, double>::value)
       if (use_tma) done = launch_rhs_dmma(N, A, rhs_only, r.num_sms, r.stream(), &info);
