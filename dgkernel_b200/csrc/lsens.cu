@@ -341,7 +341,8 @@ __global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_grad_kernel(const LsArgs
       const int x = tid + C::THREADS * b, e = min(x / NF, 7), m = x - e * NF;
       use[b] = x < 8 * NF && se[e].ok;
       g[b] = use[b] ? A.gmap[se[e].fb + m] : 0;
-      for (int d = 0; d < 4; ++d) nd[b][d] = use[b] ? A.face[d][se[e].fb + m] : 0.0;
+      // straight-sided elements: normals and Fscale are constant over a face (its first point's values)
+      for (int d = 0; d < 4; ++d) nd[b][d] = use[b] ? A.face[d][se[e].fb + (m / (NF / 4)) * (NF / 4)] : 0.0;
     }
     float ph[QF], pl[QF];
 #pragma unroll
@@ -430,7 +431,8 @@ __global__ void __launch_bounds__(LsCfg<N>::THREADS) ls_div_kernel(const LsArgs 
       const int x = tid + C::THREADS * b, e = min(x / NF, 7), m = x - e * NF;
       use[b] = x < 8 * NF && se[e].ok;
       g[b] = use[b] ? A.gmap[se[e].fb + m] : 0;
-      for (int d = 0; d < 4; ++d) nd[b][d] = use[b] ? A.face[d][se[e].fb + m] : 0.0;
+      // straight-sided elements: normals and Fscale are constant over a face (its first point's values)
+      for (int d = 0; d < 4; ++d) nd[b][d] = use[b] ? A.face[d][se[e].fb + (m / (NF / 4)) * (NF / 4)] : 0.0;
     }
     // the neighbours' rows in the active list, then their eps q
     int an[QF], node[QF];
