@@ -84,12 +84,15 @@ __global__ void __launch_bounds__(4 * kLsElems, 3) ls_sensor_kernel(const LsArgs
   const __half *W1 = sW, *b1 = W1 + kLsHid * NP, *W2 = b1 + kLsHid, *b2 = W2 + kLsHid * kLsHid, *w3 = b2 + kLsHid,
                *b3 = w3 + kLsHid;
   // Every warp walks its own groups of 8 elements (16 per 128-element tile) in rows 8 w .. 8 w + 7 of the
-  // block's buffers, with no block barrier; the state of its next group is loaded into registers while the
-  // current one is computed.
+  // block's buffers, with no block barrier; the state of its next group, the group's first element slot and
+  // (lanes 0..7) its elements' h / N are loaded into registers while the current one is computed.
   const int lane = tid & 31, w0 = (tid >> 5) * 8, nw = blockDim.x >> 5;
   const int ngroups = 16 * A.ntiles;
   constexpr int FILL = (8 * NP + 31) / 32;  // values per lane
   float fh[FILL], fl[FILL];
+  int64_t nslot = 0;
+  int nne = 0;
+  double nh = 0.0;
   auto load = [&](int gi) {
     const MTile tl = A.tiles[gi >> 4];
     const int e0 = (gi & 15) * 8;
@@ -101,13 +104,16 @@ __global__ void __launch_bounds__(4 * kLsElems, 3) ls_sensor_kernel(const LsArgs
       fh[q] = x < ne * NP ? A.uhi[base + x] : 0.f;
       fl[q] = x < ne * NP ? A.ulo[base + x] : 0.f;
     }
+    nslot = tl.elem_slot + e0;
+    nne = ne;
+    nh = lane < ne ? A.h_over_n[nslot + lane] : 0.0;
   };
   const int g0 = blockIdx.x * nw + (tid >> 5), gstep = gridDim.x * nw;
   if (g0 < ngroups) load(g0);
   for (int gi = g0; gi < ngroups; gi += gstep) {
-    const MTile tl = A.tiles[gi >> 4];
-    const int e0 = (gi & 15) * 8;
-    const int ne = max(0, min(8, tl.nelem - e0));
+    const int64_t slot0 = nslot;  // this group's first element slot, its element count and h / N (lanes 0..7)
+    const int ne = nne;
+    const double hg = nh;
 #pragma unroll
     for (int q = 0; q < FILL; ++q) {
       const int x = lane + 32 * q;
@@ -213,9 +219,10 @@ __global__ void __launch_bounds__(4 * kLsElems, 3) ls_sensor_kernel(const LsArgs
         sig = (A.mode == 3 && sg <= A.conf_lo) ? 0.0 : (double)sg;
       }
     }
+    const double hh = __shfl_sync(0xffffffffu, hg, e & 7);  // this element's h / N
     if (valid && t == 0) {
-      const int64_t slot = tl.elem_slot + e0 + (e & 7);
-      const double eps = A.eps0 * sig * A.h_over_n[slot];
+      const int64_t slot = slot0 + (e & 7);
+      const double eps = A.eps0 * sig * hh;
       A.eps[slot] = eps;
       int a = -1;
       if (eps > 0.0) {
