@@ -63,6 +63,25 @@ __device__ __forceinline__ int64_t slot_of_value(const LsArgs &A, int64_t g, int
   return -1;
 }
 
+// TF32 helpers of the network's tensor products: x = hi + lo with both parts TF32 (round to nearest), an FP16
+// weight as its exact TF32 bit pattern (0 outside the matrix), and one m16n8k8 product accumulated into d.
+__device__ __forceinline__ void ls_tf32_split(float x, uint32_t &hi, uint32_t &lo) {
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+  const float r = x - __uint_as_float(hi);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
+}
+
+__device__ __forceinline__ uint32_t ls_tf32_w(const __half *W, int i, bool in) {
+  return in ? __float_as_uint(__half2float(W[i])) : 0u;
+}
+
+__device__ __forceinline__ void ls_mma_tf32(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+  asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+               "{%0,%1,%2,%3};"
+               : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+               : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
 template <int N>
 __global__ void __launch_bounds__(4 * kLsElems, 3) ls_sensor_kernel(const LsArgs A) {
   using O = Order<N>;
@@ -184,34 +203,81 @@ __global__ void __launch_bounds__(4 * kLsElems, 3) ls_sensor_kernel(const LsArgs
         if (i < NP) sf[e * NPP + i] = (float)(uh[k] * inv);
       }
       __syncwarp();
-      const float *x = sf + e * NPP;
+      // the network on the warp's 8 elements with tensor products (mma.sync m16n8k8, TF32 operands, FP32
+      // sums): every FP16 weight is exact in TF32 and each FP32 input is split into two TF32 parts (hi + lo),
+      // so the products keep FP32-level rounding.  Rows are hidden units (two 16-row m-tiles), columns the
+      // warp's elements; lane (g = l / 4, c = l mod 4) holds units g, g + 8 (+16) of elements 2c, 2c + 1.
+      const int g = lane >> 2, c = lane & 3;
+      float o2[2][4];  // second-layer pre-activations: [m-tile][fragment]
+      {
+        float o1[2][4];
 #pragma unroll
-      for (int k = 0; k < kLsHid / 4; ++k) {
-        const int o = t + 4 * k;
-        float s0 = __half2float(b1[o]), s1 = 0.f;
-#pragma unroll
-        for (int j = 0; j + 1 < NP; j += 2) {
-          s0 = fmaf(__half2float(W1[o * NP + j]), x[j], s0);
-          s1 = fmaf(__half2float(W1[o * NP + j + 1]), x[j + 1], s1);
+        for (int mt = 0; mt < 2; ++mt) {
+          const float blo = __half2float(b1[16 * mt + g]), bhi = __half2float(b1[16 * mt + g + 8]);
+          o1[mt][0] = o1[mt][1] = blo;
+          o1[mt][2] = o1[mt][3] = bhi;
         }
-        if (NP & 1) s0 = fmaf(__half2float(W1[o * NP + NP - 1]), x[NP - 1], s0);
-        sh[e * kLsHid + o] = tanhf(s0 + s1);
-      }
-      __syncwarp();
-      float z = 0.f;
 #pragma unroll
-      for (int k = 0; k < kLsHid / 4; ++k) {
-        const int o = t + 4 * k;
-        float s0 = __half2float(b2[o]), s1 = 0.f;
+        for (int kk = 0; kk < (NP + 7) / 8; ++kk) {
+          const int j0 = 8 * kk + c, j1 = j0 + 4;
+          const float x0 = j0 < NP ? sf[(w0 + g) * NPP + j0] : 0.f, x1 = j1 < NP ? sf[(w0 + g) * NPP + j1] : 0.f;
+          uint32_t bh[2], bl[2];
+          ls_tf32_split(x0, bh[0], bl[0]);
+          ls_tf32_split(x1, bh[1], bl[1]);
 #pragma unroll
-        for (int j = 0; j < kLsHid; j += 2) {
-          s0 = fmaf(__half2float(W2[o * kLsHid + j]), sh[e * kLsHid + j], s0);
-          s1 = fmaf(__half2float(W2[o * kLsHid + j + 1]), sh[e * kLsHid + j + 1], s1);
+          for (int mt = 0; mt < 2; ++mt) {
+            const int r0 = 16 * mt + g;
+            const uint32_t a[4] = {ls_tf32_w(W1, r0 * NP + j0, j0 < NP), ls_tf32_w(W1, (r0 + 8) * NP + j0, j0 < NP),
+                                   ls_tf32_w(W1, r0 * NP + j1, j1 < NP), ls_tf32_w(W1, (r0 + 8) * NP + j1, j1 < NP)};
+            ls_mma_tf32(o1[mt], a, bh);
+            ls_mma_tf32(o1[mt], a, bl);
+          }
         }
-        z = fmaf(__half2float(w3[o]), tanhf(s0 + s1), z);
+        // first hidden layer -> shared memory [element][unit], the second layer's inputs
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+          for (int f = 0; f < 4; ++f)
+            sh[(w0 + 2 * c + (f & 1)) * kLsHid + 16 * mt + g + 8 * (f >> 1)] = tanhf(o1[mt][f]);
+        __syncwarp();
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+          const float blo = __half2float(b2[16 * mt + g]), bhi = __half2float(b2[16 * mt + g + 8]);
+          o2[mt][0] = o2[mt][1] = blo;
+          o2[mt][2] = o2[mt][3] = bhi;
+        }
+#pragma unroll
+        for (int kk = 0; kk < kLsHid / 8; ++kk) {
+          const int j0 = 8 * kk + c, j1 = j0 + 4;
+          uint32_t bh[2], bl[2];
+          ls_tf32_split(sh[(w0 + g) * kLsHid + j0], bh[0], bl[0]);
+          ls_tf32_split(sh[(w0 + g) * kLsHid + j1], bh[1], bl[1]);
+#pragma unroll
+          for (int mt = 0; mt < 2; ++mt) {
+            const int r0 = 16 * mt + g;
+            const uint32_t a[4] = {ls_tf32_w(W2, r0 * kLsHid + j0, true), ls_tf32_w(W2, (r0 + 8) * kLsHid + j0, true),
+                                   ls_tf32_w(W2, r0 * kLsHid + j1, true), ls_tf32_w(W2, (r0 + 8) * kLsHid + j1, true)};
+            ls_mma_tf32(o2[mt], a, bh);
+            ls_mma_tf32(o2[mt], a, bl);
+          }
+        }
       }
-      z += __shfl_xor_sync(0xffffffffu, z, 1);
-      z += __shfl_xor_sync(0xffffffffu, z, 2);
+      // output unit: this lane's four units for elements 2c and 2c + 1, summed over the lanes of the same c
+      float za = 0.f, zb = 0.f;
+#pragma unroll
+      for (int mt = 0; mt < 2; ++mt) {
+        const float wlo = __half2float(w3[16 * mt + g]), whi = __half2float(w3[16 * mt + g + 8]);
+        za += wlo * tanhf(o2[mt][0]) + whi * tanhf(o2[mt][2]);
+        zb += wlo * tanhf(o2[mt][1]) + whi * tanhf(o2[mt][3]);
+      }
+#pragma unroll
+      for (int m = 4; m <= 16; m <<= 1) {
+        za += __shfl_xor_sync(0xffffffffu, za, m);
+        zb += __shfl_xor_sync(0xffffffffu, zb, m);
+      }
+      const int el = e & 7;  // this thread's element: held by lane el / 2 (c = el / 2, g = 0)
+      const float zsa = __shfl_sync(0xffffffffu, za, el >> 1), zsb = __shfl_sync(0xffffffffu, zb, el >> 1);
+      const float z = (el & 1) ? zsb : zsa;
       const float sg = 1.f / (1.f + expf(-(z + __half2float(b3[0]))));
       if (sg > A.conf_lo && sg < A.conf_hi) {
         fallback = true;  // low confidence: the PP activation stands
