@@ -488,6 +488,13 @@ def run_learned(args, world, rank, local):
     dofs = runs["mlp0"]["dofs"]
     rate = {k: world * dofs / (v["ms"] * 1e-3) for k, v in runs.items()}
     fp64_rate = world * dofs / (fp64_ms * 1e-3)
+    # roofline of the composite stage on the bytes every stage moves: the tensor-core stage (state, geometry,
+    # tile-local connectivity, halo lists) and the sensor pass (the state read once, eps / active row / h / N
+    # per element); the sparse passes' bytes vary with the active set and are not counted
+    Np = 35
+    hbm, peak_kind = peaks()
+    b_alg = b_alg_tcm(4, kuhn_halo_per_elem(n, 1)) + 8 + (8 + 4 + 8) / Np
+    achieved = b_alg * dofs / (runs["mlp0"]["ms"] * 1e-3) / 1e9
     if rank == 0:
         m = runs["mlp0"]
         out = {"metric": "DOF-stage-updates/s, learned-sensor form (order 4, 48^3x6 shock)", "value": rate["mlp0"],
@@ -508,6 +515,9 @@ def run_learned(args, world, rank, local):
                           "l1_err_vs_pp_fp64": l1, "stages": m["stages"], "training_pairs": npairs,
                           "active_fraction": active, "balanced_pairs": int(len(Yb)),
                           "train_loss": [hist[0], hist[-1]], "data_s": data_s, "train_s": train_s},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                            "traffic": None, "peak_kind": peak_kind, "b_alg_per_dof": b_alg,
+                            "kernel": "composite stage (sensor pass + tensor-core stage; sparse passes not counted)"},
                "clocks": m["clk"], "gpu_launches": 7 * m["stages"]}
         print(json.dumps(out), flush=True)
 
