@@ -4,9 +4,9 @@
 // Per stage, before the tensor-core mixed stage (tcm.cu), which adds the result to its right-hand side:
 //   ls_sensor   every element: modal coefficients uhat = Vinv u (FP64, on the FP64 tensor path), the
 //               Persson-Peraire activation from log10(E_top / E), the 35 -> 32 -> 32 -> 1 network (tanh, tanh,
-//               sigmoid; FP16 weights, FP32 sums) on uhat / |uhat| with the PP fallback inside (lo, hi) and, in
-//               mode 3, outputs <= lo read as a smooth element; eps_e = eps0 sigma_e h_e / N; elements with
-//               eps_e > 0 form the active list.
+//               sigmoid; FP16 weights, FP32 sums; its hidden layers as TF32 tensor products with two-part
+//               inputs) on uhat / |uhat| with the PP fallback inside (lo, hi) and, in mode 3, outputs <= lo read
+//               as a smooth element; eps_e = eps0 sigma_e h_e / N; elements with eps_e > 0 form the active list.
 //   ls_touch    the active elements and their face neighbours are marked; ls_compact lists them (touched).
 //   ls_grad     active elements: q_d = D_d u + LIFT (Fscale n_d (uP - uM) / 2) (FP64 tensor path), stored as
 //               eps_e q_d.
