@@ -347,10 +347,12 @@ struct DmmaCfg {
   // u, resu, then 9 metrics and 4 face arrays, or the compact geometry
   static constexpr uint32_t STAGE_B = CP ? 2 * NODE_B + GEOC_B : 11 * NODE_B + 4 * FACE_B;
   static constexpr uint32_t GBUF_B = TE * NF * sizeof(T);         // gathered uP of one tile
-  static constexpr uint32_t WORK_B = 2 * GBUF_B + TE * NFS * sizeof(T) + NF * sizeof(int32_t);
+  // two gathered-uP buffers, two surface-flux buffers (a warp may start the next tile's flux while another
+  // still reads this tile's in the LIFT product), the face-point mask
+  static constexpr uint32_t WORK_B = 2 * GBUF_B + 2 * TE * NFS * sizeof(T) + NF * sizeof(int32_t);
   static constexpr int FTR = (NF / 4 + 15) & ~15;        // face-order table row: Nfp bytes rounded up to 16
   static constexpr uint32_t FTAB_B = CP ? 256 * FTR : 0;
-  static constexpr size_t SMEM = 2 * (size_t)STAGE_B + WORK_B + 8 * sizeof(uint64_t) + FTAB_B;
+  static constexpr size_t SMEM = 2 * (size_t)STAGE_B + WORK_B + 10 * sizeof(uint64_t) + FTAB_B;
   static constexpr int MINB = 2 * SMEM <= 227 * 1024 ? 2 : 1;  // co-resident CTAs the launch bounds plan for
   static constexpr int GJ = (TE * NF + 31) / 32;                  // gathers per producer lane and tile
   static_assert(NODE_B % 16 == 0 && FACE_B % 16 == 0 && GBUF_B % 16 == 0 && GEOC_B % 16 == 0,
@@ -414,12 +416,66 @@ __device__ __forceinline__ void issue_tile_b(const RhsArgs<double> &A, const Til
   if (!rhs_only) bulk_g2s(stage + C::NODE_B, A.resu + tl.node_base, nb, bar);
 }
 
+// Gather indices of one tile's face points for producer lane `lane` (points lane, lane + 32, ...), in two parts
+// so the loads can be in flight a tile ahead: dmma_gather_load issues the loads (the gather map entry; in the
+// compact form the neighbour's base and the face-order codes from the compact connectivity), and
+// dmma_gather_finish, a tile later, adds the point's node from the face-order table (compact form only).
+// Points past the tile's last element get 0 (never read).
+template <int N, bool CP>
+__device__ __forceinline__ void dmma_gather_load(const RhsArgs<double> &A, const Tile &tl, int64_t slot0, int lane,
+                                                 int32_t (&src)[DmmaCfg<N, CP>::GJ],
+                                                 uint32_t (&code)[DmmaCfg<N, CP>::GJ]) {
+  using C = DmmaCfg<N, CP>;
+  constexpr int NF = C::NF, GJ = C::GJ;
+  const int nfc = tl.nelem * NF;
+#pragma unroll
+  for (int j = 0; j < GJ; ++j) {
+    const int idx = lane + 32 * j;
+    src[j] = 0;
+    code[j] = 0;
+    if (idx < nfc) {
+      if (CP) {
+        const int e = idx / NF, f = (idx - e * NF) / (NF / 4);
+        const int32_t *cn = A.conn + (slot0 + e) * kMixedConnWords;
+        src[j] = cn[f];
+        code[j] = (uint32_t)cn[4];
+      } else {
+        src[j] = __ldcs(A.gmap + tl.face_base + idx);
+      }
+    }
+  }
+}
+
+template <int N, bool CP>
+__device__ __forceinline__ void dmma_gather_finish(const RhsArgs<double> &A, const Tile &tl, const uint8_t *sft,
+                                                   int lane, int32_t (&src)[DmmaCfg<N, CP>::GJ],
+                                                   const uint32_t (&code)[DmmaCfg<N, CP>::GJ]) {
+  if (!CP) return;
+  using C = DmmaCfg<N, CP>;
+  constexpr int NF = C::NF, GJ = C::GJ, NFP = NF / 4;
+  const int nfc = tl.nelem * NF;
+  const int ncd = min(A.ncodes, 256);
+#pragma unroll
+  for (int j = 0; j < GJ; ++j) {
+    const int idx = lane + 32 * j;
+    if (idx < nfc) {  // the point's face-order code, then the point's node in the neighbour
+      const int e = idx / NF, q = idx - e * NF, f = q / NFP, p = q - f * NFP;
+      const int cd = min((int)((code[j] >> (8 * f)) & 0xffu), ncd - 1);
+      src[j] += sft[cd * C::FTR + p];
+    }
+  }
+}
+
 // Warp-specialized CTA.  Producer warp: for tile k it reads the tile's gather map and the neighbour traces uP
 // from global memory (one batch of loads per lane), writes them to gbuf[k & 1] and signals gready; it runs up
 // to two tiles ahead, gated by gfree.  Consumer warps: wait for the TMA stage and gready, then
 // (a) [Dr;Ds;Dt] * U on the tensor path with the metrics applied in the epilogue (volume terms stay in
 // registers), (b) the Lax-Friedrichs flux of their face points, (c) LIFT * flux on the tensor path with the
-// LSERK4 update in the epilogue, streamed to HBM.  Two consumer barriers per tile.
+// LSERK4 update in the epilogue, streamed to HBM.  One consumer barrier per tile, after the flux (it also
+// AND-reduces the waits' outcome, so a timed-out wait ends every consumer there); the end of a tile is a
+// counter instead: each consumer warp adds one when it has read the slot's u and resu, and the last one issues
+// the slot's refill, so a warp goes on to the next tile without waiting for the others.  The flux buffer
+// alternates with the slot: warps are at most one tile apart (the next barrier needs all of them).
 template <int N, bool CP>
 __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
     rhs_stage_dmma_kernel(RhsArgs<double> A, int rhs_only) {
@@ -432,15 +488,17 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
   extern __shared__ __align__(128) unsigned char smem_raw[];
   char *ring = reinterpret_cast<char *>(smem_raw);
   T *gbuf = reinterpret_cast<T *>(ring + 2 * C::STAGE_B);  // [2][TE*NF] gathered uP
-  T *sf = gbuf + 2 * TE * NF;                                // surface flux of the tile
-  int *sfm = reinterpret_cast<int *>(sf + TE * NFS);
+  T *sf2 = gbuf + 2 * TE * NF;                               // [2][TE*NFS] surface flux of the tile
+  int *sfm = reinterpret_cast<int *>(sf2 + 2 * TE * NFS);
   uint64_t *bar = reinterpret_cast<uint64_t *>(sfm + NF);    // fullA[2], gready[2], gfree[2], fullB[2]
   uint64_t *full = bar, *gready = bar + 2, *gfree = bar + 4, *fullb = bar + 6;
-  uint8_t *sft = reinterpret_cast<uint8_t *>(bar + 8);  // compact form: face-order rows of C::FTR bytes
+  int *done = reinterpret_cast<int *>(bar + 8);          // [2] consumer warps done with the slot's u and resu
+  uint8_t *sft = reinterpret_cast<uint8_t *>(bar + 10);  // compact form: face-order rows of C::FTR bytes
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int G = gridDim.x;
   if (tid == 0) {
     for (int i = 0; i < 8; ++i) mbar_init(&bar[i], 1);
+    done[0] = done[1] = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   for (int i = tid; i < NF; i += C::THREADS) sfm[i] = A.fmask[i];
@@ -455,6 +513,18 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
 
   if (tid >= CONS) {
     // ---------------- producer warp: neighbour traces ----------------
+    // Software-pipelined over the CTA's tiles: while the traces of tile t are gathered, the loads of tile t + G's
+    // gather indices (from its descriptor, loaded one tile earlier) and of tile t + 2G's descriptor are in
+    // flight, so a tile costs one dependent round trip to memory instead of three.
+    Tile tl = A.tiles[blockIdx.x], tn = {};
+    int64_t sl = CP ? A.tile_slot[blockIdx.x] : 0, sn = 0;
+    if (blockIdx.x + G < A.ntiles) {
+      tn = A.tiles[blockIdx.x + G];
+      if (CP) sn = A.tile_slot[blockIdx.x + G];
+    }
+    int32_t src[GJ];
+    uint32_t code[GJ];
+    dmma_gather_load<N, CP>(A, tl, sl, lane, src, code);
     int k = 0;
     for (int t = blockIdx.x; t < A.ntiles; t += G, ++k) {
       const int s = k & 1;
@@ -462,31 +532,8 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
         if (lane == 0) atomicExch(A.status, kStatusTimeoutCode);
         return;  // consumers time out on gready and leave as well
       }
-      const Tile tl = A.tiles[t];
+      dmma_gather_finish<N, CP>(A, tl, sft, lane, src, code);
       const int nfc = tl.nelem * NF;
-      int32_t src[GJ];
-      if (CP) {  // neighbour base and face-order code of the point's face, then the point's node in it
-        constexpr int NFP = NF / 4;
-        const int64_t slot0 = A.tile_slot[t];
-        const int ncd = min(A.ncodes, 256);
-#pragma unroll
-        for (int j = 0; j < GJ; ++j) {
-          const int idx = lane + 32 * j;
-          src[j] = 0;
-          if (idx < nfc) {
-            const int e = idx / NF, q = idx - e * NF, f = q / NFP, p = q - f * NFP;
-            const int32_t *cn = A.conn + (slot0 + e) * kMixedConnWords;
-            const int cd = min((int)(((uint32_t)cn[4] >> (8 * f)) & 0xffu), ncd - 1);
-            src[j] = cn[f] + sft[cd * C::FTR + p];
-          }
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < GJ; ++j) {
-          const int idx = lane + 32 * j;
-          src[j] = idx < nfc ? __ldcs(A.gmap + tl.face_base + idx) : 0;
-        }
-      }
       T up[GJ];
 #pragma unroll
       for (int j = 0; j < GJ; ++j) {
@@ -502,6 +549,14 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
           }
         }
       }
+      // in flight with the gathers: the next tile's indices and the descriptor after it
+      Tile tnn = {};
+      int64_t snn = 0;
+      if (t + 2 * G < A.ntiles) {
+        tnn = A.tiles[t + 2 * G];
+        if (CP) snn = A.tile_slot[t + 2 * G];
+      }
+      if (t + G < A.ntiles) dmma_gather_load<N, CP>(A, tn, sn, lane, src, code);
       T *g = gbuf + s * TE * NF;
 #pragma unroll
       for (int j = 0; j < GJ; ++j) {
@@ -510,7 +565,12 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
       }
       __syncwarp();
       if (lane == 0) mbar_arrive(&gready[s]);
+      tl = tn;
+      sl = sn;
+      tn = tnn;
+      sn = snn;
     }
+    (void)sl;
     return;
   }
 
@@ -540,25 +600,28 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
       }
   }
   const T a = A.a, b = A.b, dt = A.dt;
+  constexpr int NW = CONS / 32;  // consumer warps
+  // tile descriptors in registers: this tile's and the next were loaded in earlier iterations; tile t + 2G's
+  // (read by the refills mid-tile) is loaded at the top of the iteration, before the waits
+  Tile tcur = A.tiles[blockIdx.x];
+  Tile tnext = blockIdx.x + G < A.ntiles ? A.tiles[blockIdx.x + G] : Tile{};
   int k = 0;
   for (int t = blockIdx.x; t < A.ntiles; t += G, ++k) {
     const int s = k & 1;
     const uint32_t parity = (k >> 1) & 1;
+    const bool has2 = t + 2 * G < A.ntiles;
+    Tile t2 = {};
+    int64_t slot2 = 0;
+    if (has2) {
+      t2 = A.tiles[t + 2 * G];
+      if (CP) slot2 = A.tile_slot[t + 2 * G];
+    }
+    // a wait that gives up leaves the slot unread: the tile is computed from whatever the slot holds (every
+    // index stays inside the shared-memory buffers) and the barrier after the flux ends all consumers
     const bool ready = mbar_wait_bounded(&full[s], parity, kSpinLimit) &&
                        mbar_wait_bounded(&fullb[s], parity, kSpinLimit) &&
                        mbar_wait_bounded(&gready[s], parity, kSpinLimit);
-    if (!cons_sync_and<CONS>(ready)) {
-      if (tid == 0) atomicExch(A.status, kStatusTimeoutCode);
-      // the copies in flight land before the CTA goes: this tile's and the next tile's
-      mbar_wait_bounded(&full[s], parity, kSpinLimit);
-      mbar_wait_bounded(&fullb[s], parity, kSpinLimit);
-      if (t + G < A.ntiles) {
-        mbar_wait_bounded(&full[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
-        mbar_wait_bounded(&fullb[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
-      }
-      return;
-    }
-    const Tile tl = A.tiles[t];
+    const Tile tl = tcur;
     const int ne = tl.nelem, nfc = ne * NF;
     const char *stage = ring + s * C::STAGE_B;
     const T *su = reinterpret_cast<const T *>(stage);
@@ -566,6 +629,7 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
     const T *sg = sr + TE * NP;  // per-node metrics; in the compact form the per-element geometry
     const T *sfc = reinterpret_cast<const T *>(stage + 11 * C::NODE_B);
     const T *g = gbuf + s * TE * NF;
+    T *sf = sf2 + s * TE * NFS;
 
     // (a) ur, us, ut on the tensor path; two interleaved accumulator chains per matrix
     T vol[2] = {0.0, 0.0};
@@ -617,13 +681,24 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
         sf[e * NFS + q] = (CP ? gf[3] : sfc[3 * TE * NF + idx]) * du;
       }
     }
-    cons_sync<CONS>();
+    if (!cons_sync_and<CONS>(ready)) {
+      if (tid == 0) atomicExch(A.status, kStatusTimeoutCode);
+      // the copies in flight land before the CTA goes: this tile's and the next tile's (the next tile's part B
+      // was issued when every consumer had finished the previous tile, before this barrier)
+      mbar_wait_bounded(&full[s], parity, kSpinLimit);
+      mbar_wait_bounded(&fullb[s], parity, kSpinLimit);
+      if (t + G < A.ntiles) {
+        mbar_wait_bounded(&full[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
+        mbar_wait_bounded(&fullb[s ^ 1], ((k + 1) >> 1) & 1, kSpinLimit);
+      }
+      return;
+    }
     if (tid == 0) {
       mbar_arrive(&gfree[s]);  // the gathered traces of this tile are consumed
       // the metrics and face arrays of stage s are consumed too: tile t + 2G's part A streams in during (c)
-      if (t + 2 * G < A.ntiles) {
+      if (has2) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        issue_tile_a<N, CP>(A, A.tiles[t + 2 * G], CP ? A.tile_slot[t + 2 * G] : 0, ring + s * C::STAGE_B, &full[s]);
+        issue_tile_a<N, CP>(A, t2, slot2, ring + s * C::STAGE_B, &full[s]);
       }
     }
     // (c) LIFT * flux on the tensor path, LSERK4 update in the epilogue
@@ -653,11 +728,24 @@ __global__ void __launch_bounds__(DmmaCfg<N, CP>::THREADS, DmmaCfg<N, CP>::MINB)
         }
       }
     }
-    cons_sync<CONS>();  // u and resu of stage s and the flux buffer are free
-    if (tid == 0 && t + 2 * G < A.ntiles) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue_tile_b<N, CP>(A, A.tiles[t + 2 * G], ring + s * C::STAGE_B, &fullb[s], rhs_only);
+    // this warp has read the slot's u and resu (its loads returned: their values are in the stores above); the
+    // last consumer warp to get here refills the slot's part B.  Slot s's counter is next touched by tile
+    // t + 2G, which no warp reaches before every warp passed tile t + G's barrier, after this reset.
+    __syncwarp();
+    if (lane == 0) {
+      __threadfence_block();
+      if (atomicAdd(&done[s], 1) == NW - 1) {
+        done[s] = 0;
+        __threadfence_block();
+        if (has2) {
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          issue_tile_b<N, CP>(A, t2, ring + s * C::STAGE_B, &fullb[s], rhs_only);
+        }
+      }
     }
+    // rotate the descriptors at the end of the tile, where t2's load has long returned
+    tcur = tnext;
+    tnext = t2;
   }
 }
 

@@ -277,8 +277,10 @@ int dgk_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t c
  * that owns the device-memory budget, or a time-stepping loop that cannot absorb a cudaMalloc's latency and
  * implicit synchronisation -- unlike dgk_copy_to_device, whose staging buffer grows with cudaMalloc.  More than 8 MiB of host data is rejected
  * with DGK_ERR_INVALID (split the upload).  The first call on each device resolves the array's device
- * address, so make it before any stream capture.  All calls share the array: calls that overlap on the GPU
- * race.  Errors are reported through dgk_global_error(). */
+ * address, so make it before any stream capture; the address is kept for the life of the process, so after a
+ * cudaDeviceReset (which ends the context that holds the array) the entry point must not be called again.
+ * All calls share the array: calls that overlap on the GPU race.  Errors are reported through
+ * dgk_global_error(). */
 int dgk_convert_upload_noalloc(const void *host, int32_t host_dtype, void *device_dst, int32_t dev_dtype,
                                int64_t count, void *cuda_stream);
 
